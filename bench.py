@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the XiEstimator pair count on B200: pixel-pairs/s.
+
+Default workload: the plain method on the full-survey configuration —
+160,000 seeded synthetic sightlines over ~10,000 deg^2, (r_par, r_perp)
+50x50 bins of 4 Mpc/h, HEALPix nside=64 sky cells, flat LCDM Omega_m=0.3.
+A step is one XiEstimator::run pair count over the whole catalogue (sightline
+pair search + every pixel pair binned and accumulated); pixel pairs are
+counted as the reference counts them (sum of N_i*N_j over accepted sightline
+pairs, XiEstimator.cc:149).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                  [--workload full|small|brute]
+
+N>1: launched by torchrun, one rank per GPU; every rank processes the whole
+catalogue (independent replicas, weak scaling); times are the max over ranks.
+--impl reference times the reference's CPU algorithm (the oracle port built
+with the reference's -O3 -ffast-math flags) on all host cores, rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "turbo-octo-spice_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "pixel-pairs/s on 1 B200, plain vs batched, ≤1e-6 rel err vs FP64; p50/p99"
+UNIT = "pixel-pairs/s"
+NSM = 148
+FP32_LANES_PER_SM = 128
+# FP32-pipe operations per pixel pair counted for the pair-rate roofline
+# (FMA = 1 op; MUFU and shared atomics excluded): Cartesian 6, Polar 7, brute 9.
+OPS_PER_PAIR = {"cartesian": 6, "polar": 7, "brute": 9}
+# Our kernels launched per pair-count call: 2 x cell neighbours, 2 x pair
+# expansion, the pixel-pair kernel, the cell combine (cub scan/reduce not counted).
+LAUNCHES_PER_RUN = 6
+LAUNCHES_PER_CATALOG = 3  # two sentinel fills + per-sightline prep
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", choices=["full", "small", "brute"], default="full")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=18.0, help="target CPU-baseline sample time")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self, ngpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+            self.backend = backend
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return float("nan")
+        sm = [num(r[1]) for r in rows]
+        reasons = set()
+        for r in rows:
+            for name, col in (("hw_slowdown", 5), ("hw_thermal_slowdown", 6), ("sw_thermal_slowdown", 7),
+                              ("sw_power_cap", 8)):
+                if r[col].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.nanmedian(sm)), "sm_max_mhz": num(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows), "power_w_max": float(np.nanmax([num(r[3]) for r in rows]))}
+
+
+# ---------------------------------------------------------------- workloads
+def make_workload(kind):
+    from tos_b200 import Grid, synth
+    if kind == "full":
+        los, px, meta = synth.full_survey(160000, seed=7)
+        return dict(name="plain_full_survey", los=los, px=px, scale=meta["scale"], grid=Grid.cartesian(),
+                    order=6, ops="cartesian",
+                    config={"workload": "plain method, full survey: 160000 sightlines, ~10000 deg^2, "
+                                        "(r_par,r_perp) 50x50 bins to 200 Mpc/h, HEALPix nside=64",
+                            "sightlines": 160000, "pixels": int(meta["num_pixels"]),
+                            "pixels_per_sightline_min_mean_max": meta["pixels_per_sightline"],
+                            "grid": "cartesian [0:200]*50 [0:200]*50 [3.556:3.735]*1", "healpix_order": 6,
+                            "seed": 7})
+    if kind == "small":
+        los, px, meta = synth.small_patch(2000, seed=1)
+        return dict(name="plain_small", los=los, px=px, scale=meta["scale"], grid=Grid.cartesian(), order=6,
+                    ops="cartesian",
+                    config={"workload": "plain method, small: 2000 sightlines on a 10x10 deg patch, "
+                                        "(r_par,r_perp) 50x50 bins, HEALPix nside=64",
+                            "sightlines": 2000, "pixels": int(meta["num_pixels"]), "seed": 1})
+    pts = synth.grf_grid(64, 256.0, seed=3)
+    return dict(name="brute_grf64", pts=pts, ops="brute",
+                config={"workload": "brute-force cubic grid: 64^3 GRF P(k)~k^-2, 256 Mpc/h box, "
+                                    "100 r bins 0-200 Mpc/h", "points": 262144, "seed": 3})
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_sample(W, seconds, nthreads):
+    """Time the reference algorithm (oracle, reference build flags) on a
+    bounded sample of primary cells; returns (pixel_pairs/s, sample description)."""
+    from oracle import oracle
+    if "pts" in W:
+        pts = W["pts"]
+        # rows [0, m) against all later rows: the first m*(n - (m+1)/2) pairs
+        n = len(pts)
+        m = 256
+        t = time.perf_counter()
+        oracle.brute(pts[: min(n, 4096)], 0.0, 200.0, 100, nthreads=nthreads, kind="fast")
+        dt = time.perf_counter() - t
+        npairs = min(n, 4096) * (min(n, 4096) - 1) // 2
+        rate = npairs / dt
+        sub = int(min(n, max(4096, math.sqrt(2 * rate * seconds))))
+        t = time.perf_counter()
+        oracle.brute(pts[:sub], 0.0, 200.0, 100, nthreads=nthreads, kind="fast")
+        dt = time.perf_counter() - t
+        npairs = sub * (sub - 1) // 2
+        return npairs / dt, f"all pairs of the first {sub} grid points ({npairs} pairs), {dt:.1f} s"
+    g = W["grid"]
+    costs = oracle.cell_costs(W["los"], W["order"], g.type, g.axes_array(), W["scale"], kind="fast")
+    rng = np.random.default_rng(0)
+    order = np.argsort(np.abs(costs.astype(np.float64) - np.median(costs)) + rng.uniform(0, 1e-3, len(costs)))
+    # calibrate on one median cell
+    t = time.perf_counter()
+    _, _, _, st = oracle.xi(W["los"], W["px"], W["order"], g.type, g.axes_array(), W["scale"], mode=0,
+                            nthreads=nthreads, cell_subset=np.array([order[0]]), kind="fast")
+    rate1 = st["num_pixel_pairs"] / max(time.perf_counter() - t, 1e-6)  # one thread busy
+    per_cell = float(np.median(costs))
+    ncell = int(max(2 * nthreads, min(len(costs), seconds * rate1 * nthreads / max(per_cell, 1.0))))
+    subset = np.sort(order[:ncell])
+    t = time.perf_counter()
+    _, _, _, st = oracle.xi(W["los"], W["px"], W["order"], g.type, g.axes_array(), W["scale"], mode=0,
+                            nthreads=nthreads, cell_subset=subset, kind="fast")
+    dt = time.perf_counter() - t
+    desc = (f"{ncell} of {len(costs)} occupied cells (those nearest the median cost), "
+            f"{st['num_pixel_pairs']} pixel pairs, {dt:.1f} s")
+    return st["num_pixel_pairs"] / dt, desc
+
+
+def reference_arm(args, D):
+    if D.rank != 0:
+        return
+    W = make_workload(args.workload)
+    nthreads = os.cpu_count() or 1
+    per_step = max(5.0, min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_sample(W, per_step / 2, nthreads)
+    vals, descs = [], []
+    for _ in range(args.steps):
+        v, d = cpu_sample(W, per_step, nthreads)
+        vals.append(v)
+        descs.append(d)
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": W["config"],
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                             "sample": descs[-1] + "; oracle/xi_oracle.c built with -O3 -ffast-math"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- engine arm
+def pinned_copy(a):
+    import torch
+    t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+    v = t.numpy().view(a.dtype)
+    v[...] = a
+    return t, v
+
+
+def load_traffic(name):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(path)).get(name)
+    except (OSError, ValueError):
+        return None
+
+
+def engine_arm(args, D):
+    import torch
+    import tos_b200 as T
+    W = make_workload(args.workload)
+    dev = D.local
+    eng = T.Engine(dev)
+    ops = OPS_PER_PAIR[W["ops"]]
+    if "pts" in W:
+        pts = W["pts"]
+        for _ in range(args.warmup):
+            T.brute_run(eng, pts, 0.0, 200.0, 100)
+        D.barrier()
+        clk = ClockSampler(dev)
+        clk.start()
+        ms = 0.0
+        wall = time.perf_counter()
+        for _ in range(args.steps):
+            _, _, ct, k = T.brute_run(eng, pts, 0.0, 200.0, 100)
+            ms += k
+        wall = time.perf_counter() - wall
+        clocks = clk.stop()
+        D.barrier()
+        pairs = int(ct.sum())
+        ms_max = D.max(ms)
+        value = D.world * pairs * args.steps / (ms_max / 1e3)
+        e2e_value = D.world * pairs * args.steps / D.max(wall)
+        kernel_ms = ms / args.steps
+        evaluated = pairs
+        h2d = pts.nbytes
+        d2h = 102 * 24
+        launches = 3 * args.steps
+        st = {}
+    else:
+        cat = T.Catalog(eng, W["los"], W["px"], W["order"])
+        for _ in range(args.warmup):
+            T.xi_run(eng, cat, W["grid"], W["scale"])
+        torch.cuda.synchronize(dev)
+        D.barrier()
+        clk = ClockSampler(dev)
+        clk.start()
+        ms_dev = ms_pairs = 0.0
+        for _ in range(args.steps):
+            bins, _, st = T.xi_run(eng, cat, W["grid"], W["scale"])
+            ms_dev += st["ms_device"]
+            ms_pairs += st["ms_pairs"]
+        clocks = clk.stop()
+        torch.cuda.synchronize(dev)
+        D.barrier()
+        pairs = int(st["num_pixel_pairs"])
+        ms_max = D.max(ms_dev)
+        value = D.world * pairs * args.steps / (ms_max / 1e3)
+        kernel_ms = ms_pairs / args.steps
+        evaluated = int(st["num_pixel_pairs_evaluated"])
+        launches = LAUNCHES_PER_RUN * args.steps
+        cat.close()
+        # end to end through the public API from pinned host buffers
+        _tl, los_p = pinned_copy(W["los"])
+        _tp, px_p = pinned_copy(W["px"])
+        h2d = los_p.nbytes + px_p.nbytes
+        d2h = W["grid"].nbins * 64
+        torch.cuda.synchronize(dev)
+        D.barrier()
+        wall = 0.0
+        for _ in range(max(1, args.e2e_steps)):
+            t = time.perf_counter()
+            c2 = T.Catalog(eng, los_p, px_p, W["order"])
+            b2, _, _ = T.xi_run(eng, c2, W["grid"], W["scale"])
+            c2.close()
+            wall += time.perf_counter() - t
+        assert np.array_equal(b2["num_pairs"], bins["num_pairs"])
+        e2e_value = D.world * pairs * max(1, args.e2e_steps) / D.max(wall)
+    # roofline of the pixel-pair kernel: FP32 pair-rate bound
+    sm_mhz = clocks["sm_mhz"] if clocks and clocks.get("sm_mhz") == clocks.get("sm_mhz") else 1965.0
+    peak = NSM * FP32_LANES_PER_SM * sm_mhz * 1e6 / 1e12  # tera lane-ops/s
+    achieved = evaluated * ops / (kernel_ms / 1e3) / 1e12
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": load_traffic(W["name"]),
+            "kernel": "pair_kernel" if "pts" not in W else "brute_kernel",
+            "kernel_ms": kernel_ms, "ops_per_pair": ops, "evaluated_pairs_per_launch": evaluated,
+            "peak_source": f"{NSM} SMs x {FP32_LANES_PER_SM} FP32 lanes x median SM clock under load "
+                           f"({sm_mhz:.0f} MHz); FMA counted as one op"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": dict(W["config"], parallelism=f"replicas x{D.world}",
+                           l2_note="catalogue (>1 GB) larger than L2 between steps" if "pts" not in W
+                           else "points fit in L2; all-pairs compute-bound"),
+            "roofline": roof,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches, "clocks": clocks}
+    if st:
+        line["pixel_pairs_per_step"] = pairs
+        line["pixel_pairs_used_per_step"] = int(st["num_pixel_pairs_used"])
+        line["edge_rechecks_per_step"] = int(st["num_edge_rechecks"])
+        line["ms_expand"] = st["ms_expand"]
+    if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
+        v, desc = cpu_sample(W, args.cpu_seconds, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": desc + "; oracle/xi_oracle.c built with -O3 -ffast-math"}
+    if D.rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    args = parse()
+    D = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, D)
+        else:
+            engine_arm(args, D)
+    finally:
+        D.close()
+
+
+if __name__ == "__main__":
+    main()

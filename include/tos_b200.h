@@ -1,0 +1,211 @@
+/*
+ * tos_b200.h — C ABI of the B200 pair-counting engine for the Lyman-alpha
+ * forest two-point correlation function
+ *     xi = sum w_i w_j delta_i delta_j / sum w_i w_j.
+ *
+ * This is the drop-in boundary for the pair-counting step of
+ * turbooctospice::XiEstimator (turbooctospice/XiEstimator.h:17-86,
+ * turbooctospice/XiEstimator.cc:19-305) and for the brute-force cubic-grid
+ * estimator bruteGPU (gpu/brute.h:20, gpu/brute.cu:63-225).  Paths are
+ * relative to the dmargala/turbo-octo-spice source tree.
+ *
+ * Conventions
+ *  - Every function returns tos_status; nothing throws and nothing calls exit().
+ *    tos_last_error() returns a thread-local message for the last failure.
+ *  - Plain C types only: pointers, sizes, fixed-width integers.  Host buffers
+ *    are owned by the caller; device copies are owned by the engine.
+ *  - All compute runs on the engine's CUDA device (sm_100a).  There is no CPU
+ *    fallback: on a host without that device every compute entry point fails
+ *    with TOS_ERR_NO_DEVICE.
+ *  - The library keeps no global state apart from the engines it creates and
+ *    the thread-local error string, so engines on different devices (or one
+ *    engine per host thread) are independent.
+ */
+#ifndef TOS_B200_H
+#define TOS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TOS_ABI_VERSION 1
+
+typedef enum {
+  TOS_OK = 0,
+  TOS_ERR_INVALID_ARG = 1,  /* bad pointer, size, grid or option */
+  TOS_ERR_OOM = 2,          /* device or pinned host allocation failed */
+  TOS_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+  TOS_ERR_TIMEOUT = 4,      /* a bounded device wait gave up */
+  TOS_ERR_UNSUPPORTED = 5,  /* valid request this build cannot serve */
+  TOS_ERR_NO_DEVICE = 6,    /* no sm_100 device, or the device id is out of range */
+  TOS_ERR_INTERNAL = 7      /* consistency check failed inside the engine */
+} tos_status;
+
+/* Binning coordinate type.  Same values and meaning as
+ * XiEstimator::BinningCoordinateType (XiEstimator.h:19-21):
+ *  POLAR      (r, mu, log10(lya(1+z)))         PolarGrid   (PolarGrid.h:21-23)
+ *  CARTESIAN  (r_par, r_perp, log10(lya(1+z))) CartesianGrid (CartesianGrid.h:21-23)
+ *  OBSERVING  (dloglam, theta, log10(lya(1+z))) QuasarGrid (QuasarGrid.h:21-23) */
+typedef enum { TOS_POLAR = 0, TOS_CARTESIAN = 1, TOS_OBSERVING = 2 } tos_coord_type;
+
+/* One forest pixel.  Same fields, order and types as ForestPixel
+ * (types.h:44-53): delta value, log10 wavelength, weight, comoving distance. */
+typedef struct {
+  float value, loglam, weight, distance;
+} tos_pixel;
+
+/* One sightline.  Position in radians (ra in [0, 2pi), dec in [-pi/2, pi/2]),
+ * identifiers as in Forest (types.h:56-67), and its pixels as a range of a
+ * flat pixel array.  Pixels are expected in increasing loglam order, as
+ * HDF5Delta::loadForests produces them (HDF5Delta.cc:62-73). */
+typedef struct {
+  double ra, dec;
+  int32_t forest_id, plate;
+  uint64_t pixel_offset;
+  uint32_t num_pixels, reserved;
+} tos_sightline;
+
+/* A linear axis "[min:max]*nbins" with bin width (max-min)/nbins, the binning
+ * AbsTwoPointGrid reads through getAxisMin/getAxisBinWidth/getAxisNBins
+ * (AbsTwoPointGrid.h:74-85). */
+typedef struct {
+  double min, max;
+  int32_t nbins, reserved;
+} tos_axis;
+
+/* A three-axis grid: AbsTwoPointGrid plus the coordinate type that selects
+ * CartesianGrid / PolarGrid / QuasarGrid.  Axis order is the reference's
+ * (axis1, axis2, axis3) of h5healxi (h5healxi.cc:81-86, 138-153). */
+typedef struct {
+  int32_t type; /* tos_coord_type */
+  int32_t reserved;
+  tos_axis axis[3];
+} tos_grid;
+
+/* Per-bin accumulator.  Same fields and meaning as XiBin (types.h:69-121);
+ * raw sums until tos_xibin_finalize() divides them as XiBin::finalize does. */
+typedef struct {
+  double didj, di, dj, wgt, wi, wj, z;
+  int64_t num_pairs;
+} tos_xibin;
+
+/* Counters of XiEstimator::print_stats (XiEstimator.cc:389-408) plus the
+ * engine's own work counters and device timings. */
+typedef struct {
+  uint64_t num_sightlines;
+  uint64_t num_sightline_pairs;      /* candidates j > i from neighbouring cells (depends on the cell search) */
+  uint64_t num_sightline_pairs_used; /* pairs passing cos(theta) > cos(max_ang) */
+  uint64_t num_pixels;               /* pixels of all sightlines in occupied cells */
+  uint64_t num_pixel_pairs;          /* sum of N_i*N_j over used sightline pairs */
+  uint64_t num_pixel_pairs_used;     /* pixel pairs accumulated into a bin */
+  uint64_t num_pixel_pairs_evaluated;/* pixel pairs the kernel evaluated (the rest were pruned by r_par window) */
+  uint64_t num_edge_rechecks;        /* pixel pairs re-evaluated in FP64 near a bin edge */
+  uint64_t num_index_overflow;       /* pairs whose unchecked z or theta index ran past the grid (dropped) */
+  uint64_t num_cells;                /* occupied sky cells */
+  double max_ang, cos_max_ang;       /* angular cut actually used (radians) */
+  double ms_expand;                  /* device time: sightline-pair expansion */
+  double ms_pairs;                   /* device time: pixel-pair kernel */
+  double ms_total;                   /* wall time of the call */
+  double ms_device;                  /* device time of the whole call (expansion to results) */
+} tos_xi_stats;
+
+/* Opaque handles. */
+typedef struct tos_engine tos_engine;
+typedef struct tos_catalog tos_catalog;
+
+/* ---- library / errors ---------------------------------------------------- */
+
+/* Thread-local message describing the last non-OK status on this thread. */
+const char* tos_last_error(void);
+int tos_abi_version(void);
+
+/* ---- engine -------------------------------------------------------------- */
+
+/* Create an engine on CUDA device `device`.  Replaces nothing in the reference
+ * one to one: it owns the device, streams and scratch that XiEstimator::run's
+ * ThreadPool owned on the CPU (XiEstimator.cc:31-44, ThreadPool.cc:19-25). */
+tos_status tos_engine_create(int device, tos_engine** out);
+void tos_engine_destroy(tos_engine* engine);
+
+/* ---- catalogue (sightlines + pixels resident on the device) --------------- */
+
+/* Upload sightlines and pixels, and bin sightlines into HEALPix RING cells of
+ * the given order (nside = 2^order), as HealpixBins::addItem does for every
+ * sightline in h5healxi (HealpixBins.h:31-43, h5healxi.cc:196-205).
+ * Sightline index = position in `los`; pairs are ordered by that index
+ * (XiEstimator.cc:142). Host buffers may be freed after return. */
+tos_status tos_catalog_create(tos_engine* engine, const tos_sightline* los, size_t n_los,
+                              const tos_pixel* pixels, size_t n_pixels, int healpix_order,
+                              tos_catalog** out);
+void tos_catalog_destroy(tos_catalog* catalog);
+
+/* Number of occupied sky cells (SkyBins::getNBins, SkyBins.h:53). */
+tos_status tos_catalog_num_cells(const tos_catalog* catalog, size_t* n_cells);
+/* Occupied cell ids in ascending order — the key order of
+ * XiEstimator::skybin_xis_ (XiEstimator.h:78) and of the subsample files. */
+tos_status tos_catalog_cells(const tos_catalog* catalog, int64_t* cell_ids, size_t capacity);
+/* HEALPix cell of each sightline (HealpixBins::ang2pix, HealpixBins.h:58-66). */
+tos_status tos_catalog_sightline_cells(const tos_catalog* catalog, int64_t* cells, size_t capacity);
+
+/* ---- the hot path: XiEstimator pair counting ----------------------------- */
+
+#define TOS_XI_SUBSAMPLES 0x1u   /* also return per-cell sums (skybin_xis_) */
+#define TOS_XI_EXACT      0x2u   /* evaluate every pixel pair in FP64 (validation path, slow) */
+
+/* Maximum angular scale of a grid for a transverse comoving scale:
+ * CartesianGrid::maxAngularScale (CartesianGrid.h:45-46),
+ * PolarGrid::maxAngularScale (PolarGrid.h:45-46),
+ * QuasarGrid::maxAngularScale (QuasarGrid.h:44-45). */
+tos_status tos_grid_max_angular_scale(const tos_grid* grid, double scale, double* max_ang);
+size_t tos_grid_num_bins(const tos_grid* grid);
+
+/* Run the pair count of XiEstimator::run (XiEstimator.cc:31-58) over a
+ * resident catalogue: sightline-pair search with the cut
+ * cos(theta_ij) > cos(grid.maxAngularScale(scale)) (XiEstimator.cc:121-159),
+ * then every pixel pair of every accepted sightline pair is binned and
+ * accumulated (XiEstimator.cc:161-296, types.h:77-87).
+ *   out_bins  : n_bins raw (unfinalized) sums over all cells, merged in
+ *               ascending cell order as xi_finalize_task does (XiEstimator.cc:298-305).
+ *   out_cells : NULL, or n_cells*n_bins raw per-cell sums (cell-major, cells
+ *               ascending) when flags has TOS_XI_SUBSAMPLES.
+ *   stats     : optional counters and timings. */
+tos_status tos_xi_run(tos_engine* engine, tos_catalog* catalog, const tos_grid* grid, double scale,
+                      uint32_t flags, tos_xibin* out_bins, tos_xibin* out_cells, tos_xi_stats* stats);
+
+/* XiBin::finalize (types.h:96-101) applied to n bins in place. */
+void tos_xibin_finalize(tos_xibin* bins, size_t n);
+
+/* ---- brute-force cubic-grid estimator ------------------------------------ */
+
+/* All-pairs isotropic xi(r) of bruteGPU (gpu/brute.cu:63-225) without its
+ * chunked host loop: points are (x, y, z, delta, w) rows (DataStruct,
+ * gpu/brute.cu:3-5), r = |x_i - x_j| over all i < j, bins of width
+ * (max-min)/nbins with bin 0 = underflow and nbins+1 = overflow
+ * (gpu/brute.cu:40-48).  Outputs have nbins+2 entries:
+ *   dsum[k] = sum w_i w_j d_i d_j, wsum[k] = sum w_i w_j, counts[k] = pairs.
+ * Binning is exact against the FP64 separation (FP32 fast path with an FP64
+ * recheck near bin edges). */
+tos_status tos_brute_run(tos_engine* engine, const float* points, size_t n_points, double min,
+                         double max, int nbins, double* dsum, double* wsum, uint64_t* counts,
+                         double* ms_kernel);
+
+/* ---- flat LCDM comoving distance (h5healxi.cc:123-131, 196-203) ---------- */
+
+/* Line-of-sight comoving distance in Mpc/h of a flat universe with the given
+ * Omega_matter (Omega_lambda = 1 - Omega_matter):
+ *   D_C(z) = (c / 100 km/s/Mpc) * int_0^z dz' / sqrt(Om (1+z')^3 + OL),
+ * evaluated in FP64.  Replaces cosmo::LambdaCdmUniverse::
+ * getLineOfSightComovingDistance as called at h5healxi.cc:201. */
+tos_status tos_comoving_distance(double omega_matter, const double* z, size_t n, double* out);
+/* Fill pixels[k].distance = D_C(10^(loglam - log10(1216)) - 1) on the host
+ * (h5healxi.cc:38-40, 196-203), stored as float like ForestPixel::distance. */
+tos_status tos_fill_distances(double omega_matter, tos_pixel* pixels, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOS_B200_H */

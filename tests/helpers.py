@@ -1,0 +1,76 @@
+"""Shared helpers for the tests: small catalogues and result comparison."""
+import numpy as np
+
+from tos_b200 import PIXEL_DTYPE, SIGHTLINE_DTYPE, Grid, synth
+
+FIELDS = ("didj", "di", "dj", "wgt", "wi", "wj", "z")
+
+
+def truncate(los, px, max_pixels):
+    """Keep at most max_pixels leading pixels of each sightline (compact layout)."""
+    los2 = los.copy()
+    out = []
+    off = 0
+    for s in range(len(los)):
+        n = min(int(los[s]["num_pixels"]), max_pixels)
+        o = int(los[s]["pixel_offset"])
+        out.append(px[o:o + n])
+        los2[s]["pixel_offset"] = off
+        los2[s]["num_pixels"] = n
+        off += n
+    return los2, (np.concatenate(out) if out else np.zeros(0, dtype=PIXEL_DTYPE))
+
+
+def small_catalog(n=120, seed=11, size_deg=3.0, max_pixels=None):
+    los, px, meta = synth.small_patch(n, seed=seed, size_deg=size_deg)
+    if max_pixels:
+        los, px = truncate(los, px, max_pixels)
+    return los, px, meta
+
+
+def as_matrix(bins):
+    """XiBin structured array -> (n, 8) float64 with the count in column 7."""
+    m = np.zeros((len(bins), 8))
+    for k, f in enumerate(FIELDS):
+        m[:, k] = bins[f]
+    m[:, 7] = bins["num_pairs"]
+    return m
+
+
+def assert_counts_equal(gpu, ref):
+    g = np.asarray(gpu["num_pairs"], dtype=np.int64)
+    r = np.asarray(ref["num_pairs"], dtype=np.int64)
+    bad = np.nonzero(g != r)[0]
+    assert len(bad) == 0, f"{len(bad)} bins differ in pair count, first {bad[:10]}: gpu {g[bad[:10]]} ref {r[bad[:10]]}"
+
+
+def max_rel_err(gpu, ref, floor=1e-300):
+    """Per-field max |gpu - ref| / |ref| over bins with ref != 0."""
+    out = {}
+    for f in FIELDS:
+        g, r = np.asarray(gpu[f]), np.asarray(ref[f])
+        nz = np.abs(r) > floor
+        out[f] = float(np.max(np.abs(g[nz] - r[nz]) / np.abs(r[nz]))) if nz.any() else 0.0
+        z = ~nz
+        if z.any():
+            out[f + "_abs_at_zero"] = float(np.max(np.abs(g[z])))
+    return out
+
+
+# Relative tolerance of the weighted sums against the FP64 oracle, per bin.
+REL_TOL = 1e-6
+
+
+def assert_sums_close(gpu, ref, rel=REL_TOL):
+    errs = max_rel_err(gpu, ref)
+    for f in FIELDS:
+        assert errs[f] <= rel, f"field {f}: max relative error {errs[f]:.3e} > {rel:.1e} ({errs})"
+        assert errs.get(f + "_abs_at_zero", 0.0) == 0.0, f"field {f} nonzero where the oracle is 0"
+    return errs
+
+
+GRIDS = {
+    "cartesian": Grid.cartesian(),
+    "polar": Grid.polar(),
+    "observing": Grid.observing(),
+}

@@ -1,0 +1,339 @@
+// brute.cu — all-pairs isotropic xi(r) of points (x, y, z, delta, w): the
+// computation of bruteGPU / histo_kernel (gpu/brute.cu:7-61, 63-225), redone
+// for sm_100a.
+//
+// Differences from the reference design, all in service of exactness and
+// throughput:
+//  - points stay resident in HBM (no per-chunk host copies, brute.cu:155-193);
+//  - every unordered pair i < j is visited once by a persistent sweep: a warp
+//    owns 32 consecutive points i (lane = i) and walks j = t + lane, so on a
+//    regular grid every lane has the same separation vector at the same step;
+//  - separations are binned in FP32 with an FP64 re-binning of pairs within
+//    2^-K bins of an edge, so bins equal those of the FP64 separation
+//    sqrt(dx^2+dy^2+dz^2) (the double-precision estimator of bucketxi.cc:79-98);
+//  - sums are exact: runs of equal bins are summed from FP64 prefix sums,
+//    quantised to fixed point and added with u32 shared atomics into a
+//    per-warp window, which is added to FP64 global sums when a slot fills.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine_internal.h"
+
+namespace tos {
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kBruteWarps = 16;
+constexpr int kBWords = 6;          // dsum lo/hi, wsum lo/hi, count, contributions
+constexpr int kBSplit = 20;
+constexpr uint32_t kSlotLimit = 3800;  // contributions per slot before the window is emptied
+constexpr int kRunCap = 64;            // longest run summed as one contribution
+constexpr double kMagic = 6755399441055744.0;
+constexpr long long kMagicBits = 0x4338000000000000LL;
+
+struct BruteArgs {
+  const float4* pos;      // (x, y, z, 0), n entries
+  const double2* prefix;  // n+1 exclusive prefix sums of (w*delta, w)
+  const double* wd;       // w*delta per point
+  const double* w;        // w per point
+  int n;
+  int nbins;
+  double min, max, spacing;
+  float invf, offf, nbf, nbp1f;
+  int k;
+  float mag;
+  int bits;
+  double scale[2];
+  double inv_scale[2];
+  double* out;            // [nbins+2][2] FP64 sums
+  unsigned long long* counts;  // [nbins+2]
+  unsigned long long* next;    // chunk counter
+  unsigned long long* counters;  // [0] rechecks
+};
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ long long to_fixed(double c, double scale) {
+  return __double_as_longlong(__fma_rn(c, scale, kMagic)) - kMagicBits;
+}
+
+// Histogram index of the FP64 separation: 0 below min, nbins+1 at or above
+// max, else floor((r - min) / spacing) + 1 (gpu/brute.cu:40-48 in FP64).
+__device__ __forceinline__ uint32_t exact_index(const BruteArgs& A, float4 a, float4 b) {
+  const double dx = dsub((double)a.x, (double)b.x), dy = dsub((double)a.y, (double)b.y),
+               dz = dsub((double)a.z, (double)b.z);
+  const double r = dsqrt(dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz)));
+  if (r < A.min) return 0u;
+  if (r >= A.max) return (uint32_t)A.nbins + 1u;
+  double k = floor(ddiv(dsub(r, A.min), A.spacing));
+  if (k > (double)(A.nbins - 1)) k = (double)(A.nbins - 1);
+  return (uint32_t)k + 1u;
+}
+
+__device__ void flush(const BruteArgs& A, uint32_t* win, int lane) {
+  const int S = A.nbins + 2;
+  for (int s = lane; s < S; s += 32) {
+    const uint32_t cnt = win[4 * S + s];
+    if (cnt == 0) continue;
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+      const uint32_t lo = win[(2 * f) * S + s];
+      const int hi = (int)win[(2 * f + 1) * S + s];
+      const long long q = ((long long)hi << kBSplit) + (long long)lo;
+      atomicAdd(&A.out[2 * s + f], (double)q * A.inv_scale[f]);
+    }
+    atomicAdd(&A.counts[s], (unsigned long long)cnt);
+#pragma unroll
+    for (int w = 0; w < kBWords; ++w) win[w * S + s] = 0u;
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kBruteWarps * 32, 1) brute_kernel(BruteArgs A) {
+  extern __shared__ uint32_t smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int S = A.nbins + 2;
+  uint32_t* win = smem + (size_t)warp * kBWords * S;
+  for (int k = lane; k < kBWords * S; k += 32) win[k] = 0u;
+  __syncwarp();
+  unsigned long long n_recheck = 0;
+  const int nchunks = (A.n + 31) / 32;
+  bool full = false;
+  for (;;) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(A.next, 1ull);
+    c = __shfl_sync(kFull, c, 0);
+    if (c >= (unsigned long long)nchunks) break;
+    // big chunks (long sweeps) first: chunk c covers rows i0 = 32*c'
+    const int i0 = 32 * (int)c;
+    const int i = i0 + lane;
+    const bool active = i < A.n;
+    const float4 pi = active ? A.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const double wdi = active ? A.wd[i] : 0.0, wi = active ? A.w[i] : 0.0;
+    uint32_t cur = 0xFFFFFFFFu;
+    int run_start = 0;
+    double ps0 = 0, ps1 = 0;
+    auto close_run = [&](int p_end, double2 pn) {
+      const uint32_t m = (uint32_t)(p_end - run_start);
+      const double c0 = wdi * (pn.x - ps0), c1 = wi * (pn.y - ps1);
+      const long long q0 = to_fixed(c0, A.scale[0]), q1 = to_fixed(c1, A.scale[1]);
+      const int s = (int)cur;
+      atomicAdd(&win[0 * S + s], (uint32_t)q0 & ((1u << kBSplit) - 1u));
+      atomicAdd(&win[1 * S + s], (uint32_t)(int)(q0 >> kBSplit));
+      atomicAdd(&win[2 * S + s], (uint32_t)q1 & ((1u << kBSplit) - 1u));
+      atomicAdd(&win[3 * S + s], (uint32_t)(int)(q1 >> kBSplit));
+      atomicAdd(&win[4 * S + s], m);
+      const uint32_t old = atomicAdd(&win[5 * S + s], 1u);
+      if (old >= kSlotLimit) full = true;
+    };
+    for (int t = i0 + 1; t < A.n; ++t) {
+      const int j = t + lane;
+      uint32_t key = 0xFFFFFFFFu;
+      bool recheck = false;
+      float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (active && j < A.n) {
+        pj = A.pos[j];
+        const float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y),
+                    dz = __fsub_rn(pi.z, pj.z);
+        const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+        const float tt = __fmaf_rn(sqrt_approx(r2), A.invf, A.offf);
+        const int q = __float_as_int(__fadd_rz(tt, A.mag)) - A.bits;
+        int b = (q >> A.k) + 1;
+        b = (tt < 0.f) ? 0 : ((tt >= A.nbf) ? A.nbins + 1 : b);
+        key = (uint32_t)b;
+        recheck = (((q + 1) & ((1 << A.k) - 1)) < 2) && (tt < A.nbp1f) && (tt > -1.f);
+      }
+      if (__any_sync(kFull, recheck)) {
+        if (recheck) {
+          key = exact_index(A, pi, pj);
+          ++n_recheck;
+        }
+      }
+      const bool change = (key != cur) || (cur != 0xFFFFFFFFu && j - run_start >= kRunCap);
+      if (__any_sync(kFull, change)) {
+        if (change) {
+          const int pc = min(j, A.n);
+          const double2 pn = A.prefix[pc];
+          if (cur != 0xFFFFFFFFu) close_run(j, pn);
+          cur = key;
+          run_start = j;
+          ps0 = pn.x;
+          ps1 = pn.y;
+        }
+        if (__any_sync(kFull, full)) {
+          flush(A, win, lane);
+          full = false;
+        }
+      }
+    }
+    if (cur != 0xFFFFFFFFu) {
+      const int p_end = min(A.n - 1 + lane + 1, A.n);  // last j visited was n-1 (or earlier)
+      // the sweep ended at t = n-1, so lane's last j = n-1+lane; runs only
+      // cover real points, hence end = min(n, n-1+lane+1) = n for every lane
+      close_run(p_end, A.prefix[p_end]);
+    }
+    if (__any_sync(kFull, full)) {
+      flush(A, win, lane);
+      full = false;
+    }
+  }
+  flush(A, win, lane);
+  for (int o = 16; o > 0; o >>= 1) n_recheck += __shfl_xor_sync(kFull, n_recheck, o);
+  if (lane == 0) atomicAdd(&A.counters[0], n_recheck);
+}
+
+__global__ void k_brute_prep(const float* pts, int n, float4* pos, double* wd, double* w) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const float* p = pts + 5 * (size_t)k;
+    pos[k] = make_float4(p[0], p[1], p[2], 0.f);
+    wd[k] = (double)p[4] * (double)p[3];
+    w[k] = (double)p[4];
+  }
+}
+
+// single-block exclusive scan of (wd, w) (n up to a few million: fine for a prep step)
+__global__ void k_brute_scan(const double* wd, const double* w, int n, double2* prefix) {
+  __shared__ double s0[1024], s1[1024];
+  double c0 = 0, c1 = 0;
+  if (threadIdx.x == 0) prefix[0] = make_double2(0, 0);
+  for (int base = 0; base < n; base += 1024) {
+    const int k = base + threadIdx.x;
+    s0[threadIdx.x] = k < n ? wd[k] : 0.0;
+    s1[threadIdx.x] = k < n ? w[k] : 0.0;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+      double a0 = 0, a1 = 0;
+      if (threadIdx.x >= (unsigned)d) {
+        a0 = s0[threadIdx.x - d];
+        a1 = s1[threadIdx.x - d];
+      }
+      __syncthreads();
+      s0[threadIdx.x] += a0;
+      s1[threadIdx.x] += a1;
+      __syncthreads();
+    }
+    if (k < n) prefix[k + 1] = make_double2(c0 + s0[threadIdx.x], c1 + s1[threadIdx.x]);
+    c0 += s0[1023];
+    c1 += s1[1023];
+    __syncthreads();
+  }
+}
+
+}  // namespace
+}  // namespace tos
+
+using namespace tos;
+
+extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n_points, double min,
+                                    double max, int nbins, double* dsum, double* wsum,
+                                    uint64_t* counts, double* ms_kernel) {
+  if (!e || !points || !dsum || !wsum || !counts) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (n_points < 2 || n_points > (1u << 28)) return fail(TOS_ERR_INVALID_ARG, "need 2 <= n < 2^28 points");
+  if (nbins <= 0 || nbins > 4096) return fail(TOS_ERR_INVALID_ARG, "nbins must be in [1, 4096]");
+  if (!(max > min) || !std::isfinite(min) || !std::isfinite(max))
+    return fail(TOS_ERR_INVALID_ARG, "need finite min < max");
+  std::lock_guard<std::mutex> lock(e->mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(e->device);
+  struct Restore {
+    int d;
+    ~Restore() { cudaSetDevice(d); }
+  } restore{prev};
+  const int n = (int)n_points;
+  cudaStream_t st = e->stream;
+  DevBuf<float> d_pts;
+  DevBuf<float4> d_pos;
+  DevBuf<double> d_wd, d_w, d_out;
+  DevBuf<double2> d_prefix;
+  DevBuf<unsigned long long> d_counts, d_misc;
+  TOS_TRY(d_pts.alloc((size_t)n * 5));
+  TOS_TRY(d_pos.alloc(n));
+  TOS_TRY(d_wd.alloc(n));
+  TOS_TRY(d_w.alloc(n));
+  TOS_TRY(d_prefix.alloc((size_t)n + 1));
+  TOS_TRY(d_out.alloc((size_t)(nbins + 2) * 2));
+  TOS_TRY(d_counts.alloc(nbins + 2));
+  TOS_TRY(d_misc.alloc(4));
+  TOS_CUDA_TRY(cudaMemcpyAsync(d_pts.p, points, (size_t)n * 5 * sizeof(float),
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemsetAsync(d_out.p, 0, (size_t)(nbins + 2) * 2 * 8, st));
+  TOS_CUDA_TRY(cudaMemsetAsync(d_counts.p, 0, (size_t)(nbins + 2) * 8, st));
+  TOS_CUDA_TRY(cudaMemsetAsync(d_misc.p, 0, 32, st));
+  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_pts.p, n, d_pos.p, d_wd.p, d_w.p);
+  k_brute_scan<<<1, 1024, 0, st>>>(d_wd.p, d_w.p, n, d_prefix.p);
+  TOS_CUDA_TRY(cudaGetLastError());
+  // bounds of |w*delta| and |w| for the fixed-point scale
+  std::vector<float> hp((size_t)n * 5);
+  std::memcpy(hp.data(), points, hp.size() * sizeof(float));
+  double mwd = 1e-300, mw = 1e-300;
+  for (int k = 0; k < n; ++k) {
+    const double wv = hp[5 * (size_t)k + 4], dv = hp[5 * (size_t)k + 3];
+    if (!std::isfinite(wv) || !std::isfinite(dv) || !std::isfinite(hp[5 * (size_t)k]) ||
+        !std::isfinite(hp[5 * (size_t)k + 1]) || !std::isfinite(hp[5 * (size_t)k + 2]))
+      return fail(TOS_ERR_INVALID_ARG, "points must be finite");
+    mwd = std::max(mwd, std::fabs(wv * dv));
+    mw = std::max(mw, std::fabs(wv));
+  }
+  BruteArgs A{};
+  A.pos = d_pos.p;
+  A.prefix = d_prefix.p;
+  A.wd = d_wd.p;
+  A.w = d_w.p;
+  A.n = n;
+  A.nbins = nbins;
+  A.min = min;
+  A.max = max;
+  A.spacing = (max - min) / nbins;
+  A.invf = (float)(1.0 / A.spacing);
+  A.offf = (float)(-min / A.spacing);
+  A.nbf = (float)nbins;
+  A.nbp1f = (float)nbins + 1.0f;
+  int bl = 0;
+  for (uint32_t v = (uint32_t)nbins + 2; v; v >>= 1) ++bl;
+  A.k = std::max(0, std::min(13, 21 - bl));
+  A.mag = std::ldexp(1.5f, 23 - A.k);
+  std::memcpy(&A.bits, &A.mag, 4);
+  const double per[2] = {mwd * kRunCap * mwd, mw * kRunCap * mw};
+  for (int f = 0; f < 2; ++f) {
+    const int F = (int)std::floor(38.0 - std::log2(per[f]));
+    A.scale[f] = std::ldexp(1.0, F);
+    A.inv_scale[f] = std::ldexp(1.0, -F);
+  }
+  A.out = d_out.p;
+  A.counts = d_counts.p;
+  A.next = d_misc.p;
+  A.counters = d_misc.p + 1;
+  const size_t smem = (size_t)kBruteWarps * kBWords * (nbins + 2) * sizeof(uint32_t);
+  TOS_CUDA_TRY(cudaFuncSetAttribute(brute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
+  brute_kernel<<<e->num_sms, kBruteWarps * 32, smem, st>>>(A);
+  TOS_CUDA_TRY(cudaGetLastError());
+  TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
+  std::vector<double> out((size_t)(nbins + 2) * 2);
+  std::vector<unsigned long long> cnt(nbins + 2);
+  TOS_CUDA_TRY(cudaMemcpyAsync(out.data(), d_out.p, out.size() * 8, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cnt.data(), d_counts.p, cnt.size() * 8, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int b = 0; b < nbins + 2; ++b) {
+    dsum[b] = out[2 * b];
+    wsum[b] = out[2 * b + 1];
+    counts[b] = cnt[b];
+  }
+  if (ms_kernel) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev[4], e->ev[5]);
+    *ms_kernel = ms;
+  }
+  return TOS_OK;
+}

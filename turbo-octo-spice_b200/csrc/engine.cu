@@ -1,0 +1,915 @@
+// engine.cu — engine, catalogue upload, sightline-pair expansion and the
+// XiEstimator run entry point of the C ABI (include/tos_b200.h).
+#include <cub/cub.cuh>
+
+#include <memory>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "engine_internal.h"
+#include "healpix.h"
+#include "xi_kernels.cuh"
+
+namespace tos {
+
+namespace {
+thread_local std::string g_error;
+}  // namespace
+
+void set_error(const std::string& msg) { g_error = msg; }
+tos_status fail(tos_status s, const std::string& msg) {
+  g_error = msg;
+  return s;
+}
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// ---- catalogue preparation -------------------------------------------------
+
+__global__ void k_fill(float* p, size_t n, float v) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x)
+    p[k] = v;
+}
+
+// One warp per sightline: scatter pixels into the padded coordinate arrays,
+// w*delta (exact product of two floats in double), weights; exclusive prefix
+// sums of (w*delta, w, loglam); coordinate ranges; sortedness.
+__global__ void k_prep(const tos_pixel* raw, const uint64_t* off, const uint32_t* npix,
+                       size_t n_los, float* dist_pad, float* loglam_pad, double* wd, float* w,
+                       double4* prefix, float4* range, unsigned int* flags,
+                       unsigned long long* maxbits) {
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t s = warp; s < n_los; s += nwarps) {
+    const uint64_t o = off[s];
+    const uint32_t n = npix[s];
+    const uint64_t po = o + (uint64_t)kPad * (s + 1);
+    double4* pre = prefix + o + s;
+    double c0 = 0, c1 = 0, c2 = 0;
+    float dmin = INFINITY, dmax = -INFINITY, lmin = INFINITY, lmax = -INFINITY;
+    double mwd = 0, mw = 0, ml = 0, md = 0;
+    bool unsorted = false;
+    if (lane == 0) pre[0] = make_double4(0, 0, 0, 0);
+    for (uint32_t b = 0; b < n; b += 32) {
+      const uint32_t k = b + lane;
+      double v0 = 0, v1 = 0, v2 = 0;
+      if (k < n) {
+        const tos_pixel px = raw[o + k];
+        dist_pad[po + k] = px.distance;
+        loglam_pad[po + k] = px.loglam;
+        v0 = (double)px.weight * (double)px.value;
+        v1 = (double)px.weight;
+        v2 = (double)px.loglam;
+        wd[o + k] = v0;
+        w[o + k] = px.weight;
+        dmin = fminf(dmin, px.distance);
+        dmax = fmaxf(dmax, px.distance);
+        lmin = fminf(lmin, px.loglam);
+        lmax = fmaxf(lmax, px.loglam);
+        mwd = fmax(mwd, fabs(v0));
+        mw = fmax(mw, fabs(v1));
+        ml = fmax(ml, fabs(v2));
+        md = fmax(md, fabs((double)px.distance));
+        if (k + 1 < n) {
+          const tos_pixel nx = raw[o + k + 1];
+          if (!(nx.distance >= px.distance) || !(nx.loglam >= px.loglam)) unsorted = true;
+        }
+      }
+      // inclusive warp scan, in order, of the three sums
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const double u0 = __shfl_up_sync(kFull, v0, d), u1 = __shfl_up_sync(kFull, v1, d),
+                     u2 = __shfl_up_sync(kFull, v2, d);
+        if (lane >= d) {
+          v0 += u0;
+          v1 += u1;
+          v2 += u2;
+        }
+      }
+      if (k < n) pre[k + 1] = make_double4(c0 + v0, c1 + v1, c2 + v2, 0);
+      c0 += __shfl_sync(kFull, v0, 31);
+      c1 += __shfl_sync(kFull, v1, 31);
+      c2 += __shfl_sync(kFull, v2, 31);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      dmin = fminf(dmin, __shfl_xor_sync(kFull, dmin, d));
+      dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, d));
+      lmin = fminf(lmin, __shfl_xor_sync(kFull, lmin, d));
+      lmax = fmaxf(lmax, __shfl_xor_sync(kFull, lmax, d));
+      mwd = fmax(mwd, __shfl_xor_sync(kFull, mwd, d));
+      mw = fmax(mw, __shfl_xor_sync(kFull, mw, d));
+      ml = fmax(ml, __shfl_xor_sync(kFull, ml, d));
+      md = fmax(md, __shfl_xor_sync(kFull, md, d));
+    }
+    unsorted = __any_sync(kFull, unsorted);
+    if (lane == 0) {
+      range[s] = make_float4(dmin, dmax, lmin, lmax);
+      if (unsorted) atomicOr(flags, 1u);
+      // non-negative doubles order like their bit patterns
+      atomicMax(&maxbits[0], (unsigned long long)__double_as_longlong(mwd));
+      atomicMax(&maxbits[1], (unsigned long long)__double_as_longlong(mw));
+      atomicMax(&maxbits[2], (unsigned long long)__double_as_longlong(ml));
+      atomicMax(&maxbits[3], (unsigned long long)__double_as_longlong(md));
+    }
+  }
+}
+
+// ---- sightline-pair expansion ----------------------------------------------
+
+// Conservative cell neighbours: cells A, B can hold a sightline pair within
+// max_ang only if the angle between their caps' centres is at most
+// max_ang + r_A + r_B (caps bound every member).
+__global__ void k_cell_neighbours(const double4* cap, uint32_t n_cells, double max_ang,
+                                  const uint32_t* start, uint32_t* count, uint32_t* out) {
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < n_cells;
+       a += gridDim.x * blockDim.x) {
+    const double4 ca = cap[a];
+    uint32_t n = 0;
+    uint32_t o = out ? start[a] : 0;
+    for (uint32_t b = 0; b < n_cells; ++b) {
+      const double4 cb = cap[b];
+      const double lim = max_ang + ca.w + cb.w + 1e-9;
+      bool near;
+      if (lim >= 3.14159) {
+        near = true;
+      } else {
+        const double dot = ca.x * cb.x + ca.y * cb.y + ca.z * cb.z;
+        near = dot >= cos(lim) - 1e-12;
+      }
+      if (near) {
+        if (out) out[o + n] = b;
+        ++n;
+      }
+    }
+    if (!out) count[a] = n;
+  }
+}
+
+// One warp per primary sightline (in cell order).  Pass 1 (items == null)
+// counts accepted pairs and candidates; pass 2 writes the accepted pairs at
+// their offsets in a fixed order (neighbour cells ascending, j ascending).
+// Mirrors skybin_xi_task's loop (XiEstimator.cc:130-152): skip j <= i, cut
+// cos(theta) <= cos_max.
+__global__ void k_expand(const uint32_t* members, uint32_t n_members, const uint32_t* cell_idx,
+                         const uint32_t* cell_start, const uint32_t* nb_start, const uint32_t* nb,
+                         const double4* trig, const uint32_t* npix, double cos_max,
+                         uint32_t* cnt, unsigned long long* cand, unsigned long long* cell_pairs,
+                         const uint32_t* item_off, uint32_t* item_i, uint32_t* item_j,
+                         double* item_c, uint32_t* item_sep, int coord, double theta_min,
+                         double theta_inv, unsigned long long* sep_flagged) {
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t p = warp; p < n_members; p += nwarps) {
+    const uint32_t i = members[p];
+    const uint32_t ca = cell_idx[i];
+    const double4 ti = trig[i];
+    const SkyTrig si{ti.x, ti.y, ti.z, ti.w};
+    uint32_t n_acc = 0;
+    unsigned long long n_cand = 0, n_pairs = 0;
+    uint32_t o = item_i ? item_off[p] : 0;
+    for (uint32_t q = nb_start[ca]; q < nb_start[ca + 1]; ++q) {
+      const uint32_t cb = nb[q];
+      const uint32_t b0 = cell_start[cb], b1 = cell_start[cb + 1];
+      for (uint32_t base = b0; base < b1; base += 32) {
+        const uint32_t k = base + lane;
+        bool cnd = false, acc = false;
+        double c = 0;
+        uint32_t j = 0;
+        if (k < b1) {
+          j = members[k];
+          if (j > i) {
+            cnd = true;
+            const double4 tj = trig[j];
+            c = ref_cos_sep(si, SkyTrig{tj.x, tj.y, tj.z, tj.w});
+            acc = !(c <= cos_max);
+          }
+        }
+        const unsigned mc = __ballot_sync(kFull, cnd), ma = __ballot_sync(kFull, acc);
+        n_cand += __popc(mc);
+        if (acc) n_pairs += npix[j];
+        if (item_i && acc) {
+          const uint32_t at = o + n_acc + __popc(ma & ((1u << lane) - 1u));
+          item_i[at] = i;
+          item_j[at] = j;
+          item_c[at] = c;
+          if (coord == TOS_OBSERVING) {
+            // theta index of XiEstimator.cc:166, 273 (acos, unchecked)
+            const double th = acos(c);
+            const double t = dmul(dsub(th, theta_min), theta_inv);
+            item_sep[at] = ref_u32(t);
+            const double fr = t - floor(t);
+            if (fr < 1e-9 || fr > 1.0 - 1e-9) {
+              const unsigned long long slot = atomicAdd(&sep_flagged[0], 1ull);
+              if (slot < 4096) sep_flagged[1 + slot] = at;
+            }
+          }
+        }
+        n_acc += __popc(ma);
+      }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) n_pairs += __shfl_xor_sync(kFull, n_pairs, d);
+    if (!item_i && lane == 0) {
+      cnt[p] = n_acc;
+      cand[p] = n_cand;
+      atomicAdd(&cell_pairs[ca], n_pairs * (unsigned long long)npix[i]);
+    }
+  }
+}
+
+// ---- results ----------------------------------------------------------------
+
+// Per bin: convert every cell's fixed-point sums to double and add them in
+// ascending cell order (the order of xi_finalize_task, XiEstimator.cc:298-305).
+__global__ void k_combine(const long long* acc, uint32_t n_cells, uint32_t nb, double4 inv_a,
+                          double4 inv_b, tos_xibin* out, tos_xibin* cells_out) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const double inv[7] = {inv_a.x, inv_a.y, inv_a.z, inv_a.w, inv_b.x, inv_b.y, inv_b.z};
+    double s[7] = {0, 0, 0, 0, 0, 0, 0};
+    long long n = 0;
+    for (uint32_t c = 0; c < n_cells; ++c) {
+      const long long* a = acc + ((size_t)c * nb + b) * 8;
+      double v[7];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+        v[k] = (double)a[k] * inv[k];
+        s[k] += v[k];
+      }
+      n += a[7];
+      if (cells_out) {
+        tos_xibin x;
+        x.didj = v[0];
+        x.di = v[1];
+        x.dj = v[2];
+        x.wgt = v[3];
+        x.wi = v[4];
+        x.wj = v[5];
+        x.z = v[6];
+        x.num_pairs = a[7];
+        cells_out[(size_t)c * nb + b] = x;
+      }
+    }
+    tos_xibin x;
+    x.didj = s[0];
+    x.di = s[1];
+    x.dj = s[2];
+    x.wgt = s[3];
+    x.wi = s[4];
+    x.wj = s[5];
+    x.z = s[6];
+    x.num_pairs = n;
+    out[b] = x;
+  }
+}
+
+int grid_for(const tos_engine* e, size_t work, int block) {
+  size_t g = (work + block - 1) / block;
+  size_t cap = (size_t)e->num_sms * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// Smallest float r >= 0 with ref_u32((r - min) * inv) >= n: every
+// |fl32(x1 - x2)| >= r is rejected by the first-axis check.
+float first_axis_limit(double min, double inv, uint32_t n) {
+  auto rejected = [&](float r) { return ref_u32(dmul(dsub((double)r, min), inv)) >= n; };
+  float hi = (float)(min + (double)n / inv);
+  if (!(hi > 0)) hi = 1.0f;
+  int guard = 0;
+  while (!rejected(hi) && guard++ < 200) hi = hi * 2.0f + 1.0f;
+  if (!rejected(hi)) return INFINITY;
+  float lo = 0.0f;
+  if (rejected(lo)) return 0.0f;
+  // bisection over the ordered float bit patterns (both non-negative)
+  uint32_t a, b;
+  std::memcpy(&a, &lo, 4);
+  std::memcpy(&b, &hi, 4);
+  while (b - a > 1) {
+    const uint32_t m = a + (b - a) / 2;
+    float fm;
+    std::memcpy(&fm, &m, 4);
+    if (rejected(fm))
+      b = m;
+    else
+      a = m;
+  }
+  float r;
+  std::memcpy(&r, &b, 4);
+  return r;
+}
+
+int bitlen(uint32_t v) {
+  int b = 0;
+  while (v) {
+    ++b;
+    v >>= 1;
+  }
+  return b;
+}
+
+bool is_pow2(double v) {
+  if (!(v > 0) || !std::isfinite(v)) return false;
+  int e;
+  const double m = std::frexp(v, &e);
+  return m == 0.5;
+}
+
+}  // namespace
+
+// ---- grid helpers -----------------------------------------------------------
+
+tos_status check_grid(const tos_grid* g) {
+  if (!g) return fail(TOS_ERR_INVALID_ARG, "grid is null");
+  if (g->type != TOS_POLAR && g->type != TOS_CARTESIAN && g->type != TOS_OBSERVING)
+    return fail(TOS_ERR_INVALID_ARG, "unknown coordinate type");
+  for (int k = 0; k < 3; ++k) {
+    const tos_axis& a = g->axis[k];
+    if (a.nbins <= 0 || a.nbins > 32767)
+      return fail(TOS_ERR_INVALID_ARG, "axis bins must be in [1, 32767]");
+    if (!std::isfinite(a.min) || !std::isfinite(a.max) || !(a.max > a.min))
+      return fail(TOS_ERR_INVALID_ARG, "axis needs finite min < max");
+  }
+  const double total = (double)g->axis[0].nbins * g->axis[1].nbins * g->axis[2].nbins;
+  if (total > 1.0e7) return fail(TOS_ERR_UNSUPPORTED, "grid has more than 1e7 bins");
+  return TOS_OK;
+}
+
+double max_angular_scale(const tos_grid& g, double scale) {
+  switch (g.type) {
+    case TOS_CARTESIAN: return axis_high(g.axis[1]) / scale;  // CartesianGrid.h:46
+    case TOS_POLAR:  // PolarGrid.h:46
+      return axis_high(g.axis[0]) * std::sqrt(1.0 - g.axis[1].min * g.axis[1].min) / scale;
+    default: return axis_high(g.axis[1]);  // QuasarGrid.h:45 (no scaling)
+  }
+}
+
+}  // namespace tos
+
+using namespace tos;
+
+// ============================================================================
+// C ABI
+// ============================================================================
+
+extern "C" {
+
+const char* tos_last_error(void) { return tos::g_error.c_str(); }
+int tos_abi_version(void) { return TOS_ABI_VERSION; }
+
+tos_status tos_engine_create(int device, tos_engine** out) {
+  if (!out) return fail(TOS_ERR_INVALID_ARG, "out is null");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return fail(TOS_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= n) return fail(TOS_ERR_NO_DEVICE, "device id out of range");
+  cudaDeviceProp prop;
+  TOS_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return fail(TOS_ERR_NO_DEVICE, "device is not sm_100 (Blackwell): " + std::string(prop.name));
+  auto* e = new tos_engine();
+  e->device = device;
+  e->num_sms = prop.multiProcessorCount;
+  DeviceGuard g(device);
+  if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete e;
+    return fail(TOS_ERR_CUDA, "stream creation failed");
+  }
+  for (auto& ev : e->ev) cudaEventCreate(&ev);
+  *out = e;
+  return TOS_OK;
+}
+
+void tos_engine_destroy(tos_engine* e) {
+  if (!e) return;
+  {
+    DeviceGuard g(e->device);
+    cudaStreamSynchronize(e->stream);
+    for (auto& ev : e->ev) cudaEventDestroy(ev);
+    cudaStreamDestroy(e->stream);
+  }
+  delete e;
+}
+
+tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_los,
+                              const tos_pixel* pixels, size_t n_pixels, int order,
+                              tos_catalog** out) {
+  if (!e || !out) return fail(TOS_ERR_INVALID_ARG, "engine/out is null");
+  *out = nullptr;
+  if (n_los == 0 || !los) return fail(TOS_ERR_INVALID_ARG, "no sightlines");
+  if (n_los >= 0xFFFFFFF0ull) return fail(TOS_ERR_UNSUPPORTED, "too many sightlines");
+  if (order < 0 || order > 13) return fail(TOS_ERR_INVALID_ARG, "healpix order must be in [0, 13]");
+  if (n_pixels > 0 && !pixels) return fail(TOS_ERR_INVALID_ARG, "pixels is null");
+  std::lock_guard<std::mutex> lock(e->mu);
+  DeviceGuard g(e->device);
+  std::unique_ptr<tos_catalog> cat(new tos_catalog());
+  cat->eng = e;
+  cat->n_los = n_los;
+  cat->order = order;
+  cat->nside = (int64_t)1 << order;
+  // --- host index: pixel ranges, trig, cells
+  cat->npix.resize(n_los);
+  cat->off.resize(n_los);
+  bool contiguous = true;
+  uint64_t total = 0;
+  for (size_t s = 0; s < n_los; ++s) {
+    const tos_sightline& l = los[s];
+    if (l.pixel_offset > n_pixels || (uint64_t)l.num_pixels > n_pixels - l.pixel_offset)
+      return fail(TOS_ERR_INVALID_ARG, "sightline " + std::to_string(s) + " pixel range out of bounds");
+    if (!std::isfinite(l.ra) || !std::isfinite(l.dec))
+      return fail(TOS_ERR_INVALID_ARG, "sightline " + std::to_string(s) + " has non-finite position");
+    cat->npix[s] = l.num_pixels;
+    cat->off[s] = total;
+    if (l.pixel_offset != total) contiguous = false;
+    total += l.num_pixels;
+    cat->max_np = std::max(cat->max_np, l.num_pixels);
+  }
+  cat->n_pix = total;
+  std::vector<double4> trig(n_los);
+  cat->cell_of.resize(n_los);
+  for (size_t s = 0; s < n_los; ++s) {
+    // SkyObject's cached sines and cosines (types.h:20-26)
+    trig[s] = make_double4(std::sin(los[s].dec), std::cos(los[s].dec), std::sin(los[s].ra),
+                           std::cos(los[s].ra));
+    cat->cell_of[s] = healpix_radec2pix(cat->nside, los[s].ra, los[s].dec);
+  }
+  cat->cells = cat->cell_of;
+  std::sort(cat->cells.begin(), cat->cells.end());
+  cat->cells.erase(std::unique(cat->cells.begin(), cat->cells.end()), cat->cells.end());
+  const size_t nc = cat->cells.size();
+  cat->cell_idx.resize(n_los);
+  std::vector<uint32_t> ccount(nc + 1, 0);
+  for (size_t s = 0; s < n_los; ++s) {
+    const uint32_t ci = (uint32_t)(std::lower_bound(cat->cells.begin(), cat->cells.end(),
+                                                    cat->cell_of[s]) - cat->cells.begin());
+    cat->cell_idx[s] = ci;
+    ccount[ci + 1]++;
+  }
+  cat->cell_start.assign(nc + 1, 0);
+  for (size_t c = 0; c < nc; ++c) cat->cell_start[c + 1] = cat->cell_start[c] + ccount[c + 1];
+  cat->members.resize(n_los);
+  {
+    std::vector<uint32_t> fill(cat->cell_start.begin(), cat->cell_start.end() - 1);
+    for (size_t s = 0; s < n_los; ++s) cat->members[fill[cat->cell_idx[s]]++] = (uint32_t)s;
+  }
+  // cell caps: unit centre and angular radius bounding every member
+  std::vector<double4> caps(nc);
+  for (size_t c = 0; c < nc; ++c) {
+    double x = 0, y = 0, z = 0;
+    for (uint32_t k = cat->cell_start[c]; k < cat->cell_start[c + 1]; ++k) {
+      const double4 t = trig[cat->members[k]];
+      x += t.y * t.w;
+      y += t.y * t.z;
+      z += t.x;
+    }
+    double nrm = std::sqrt(x * x + y * y + z * z);
+    if (!(nrm > 0)) {
+      const double4 t = trig[cat->members[cat->cell_start[c]]];
+      x = t.y * t.w, y = t.y * t.z, z = t.x, nrm = 1.0;
+    }
+    x /= nrm, y /= nrm, z /= nrm;
+    double rad = 0;
+    for (uint32_t k = cat->cell_start[c]; k < cat->cell_start[c + 1]; ++k) {
+      const double4 t = trig[cat->members[k]];
+      double d = x * t.y * t.w + y * t.y * t.z + z * t.x;
+      d = std::max(-1.0, std::min(1.0, d));
+      rad = std::max(rad, std::acos(d));
+    }
+    caps[c] = make_double4(x, y, z, rad * (1 + 1e-9) + 1e-12);
+  }
+  // --- device buffers
+  TOS_TRY(cat->d_trig.alloc(n_los));
+  TOS_TRY(cat->d_cap.alloc(nc));
+  TOS_TRY(cat->d_cell_idx.alloc(n_los));
+  TOS_TRY(cat->d_cell_start.alloc(nc + 1));
+  TOS_TRY(cat->d_members.alloc(n_los));
+  TOS_TRY(cat->d_npix.alloc(n_los));
+  TOS_TRY(cat->d_off.alloc(n_los));
+  TOS_TRY(cat->d_raw.alloc(total));
+  const size_t padded = total + (size_t)kPad * (n_los + 1);
+  TOS_TRY(cat->d_dist_pad.alloc(padded));
+  TOS_TRY(cat->d_loglam_pad.alloc(padded));
+  TOS_TRY(cat->d_wd.alloc(total));
+  TOS_TRY(cat->d_w.alloc(total));
+  TOS_TRY(cat->d_prefix.alloc(total + n_los));
+  TOS_TRY(cat->d_range.alloc(n_los));
+  TOS_TRY(cat->d_flags.alloc(1));
+  TOS_TRY(cat->d_maxes.alloc(4));
+  cudaStream_t st = e->stream;
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_trig.p, trig.data(), n_los * sizeof(double4),
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cap.p, caps.data(), nc * sizeof(double4),
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cell_idx.p, cat->cell_idx.data(), n_los * 4,
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cell_start.p, cat->cell_start.data(), (nc + 1) * 4,
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_members.p, cat->members.data(), n_los * 4,
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_npix.p, cat->npix.data(), n_los * 4,
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_off.p, cat->off.data(), n_los * 8,
+                               cudaMemcpyHostToDevice, st));
+  if (total > 0) {
+    if (contiguous) {
+      TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_raw.p, pixels + los[0].pixel_offset,
+                                   total * sizeof(tos_pixel), cudaMemcpyHostToDevice, st));
+    } else {
+      for (size_t s = 0; s < n_los; ++s)
+        if (los[s].num_pixels)
+          TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_raw.p + cat->off[s], pixels + los[s].pixel_offset,
+                                       (size_t)los[s].num_pixels * sizeof(tos_pixel),
+                                       cudaMemcpyHostToDevice, st));
+    }
+  }
+  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_flags.p, 0, sizeof(unsigned int), st));
+  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_maxes.p, 0, 4 * sizeof(double), st));
+  k_fill<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_dist_pad.p, padded, kSentinel);
+  k_fill<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_loglam_pad.p, padded, kSentinel);
+  k_prep<<<grid_for(e, n_los * 32, 256), 256, 0, st>>>(
+      cat->d_raw.p, cat->d_off.p, cat->d_npix.p, n_los, cat->d_dist_pad.p, cat->d_loglam_pad.p,
+      cat->d_wd.p, cat->d_w.p, cat->d_prefix.p, cat->d_range.p, cat->d_flags.p,
+      (unsigned long long*)cat->d_maxes.p);
+  TOS_CUDA_TRY(cudaGetLastError());
+  unsigned int flags = 0;
+  double maxes[4];
+  TOS_CUDA_TRY(cudaMemcpyAsync(&flags, cat->d_flags.p, 4, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(maxes, cat->d_maxes.p, 32, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  cat->sorted = (flags & 1u) == 0;
+  cat->max_abs_wd = maxes[0];
+  cat->max_w = maxes[1];
+  cat->max_l = maxes[2];
+  cat->max_d = maxes[3];
+  if (!std::isfinite(cat->max_abs_wd) || !std::isfinite(cat->max_w) ||
+      !std::isfinite(cat->max_l) || !std::isfinite(cat->max_d))
+    return fail(TOS_ERR_INVALID_ARG,
+                "pixels must have finite value, weight, loglam and distance (filter them as "
+                "HDF5Delta::loadForests does)");
+  // the raw copy is no longer needed
+  cat->d_raw.release();
+  *out = cat.release();
+  return TOS_OK;
+}
+
+void tos_catalog_destroy(tos_catalog* c) {
+  if (!c) return;
+  DeviceGuard g(c->eng->device);
+  cudaStreamSynchronize(c->eng->stream);
+  delete c;
+}
+
+tos_status tos_catalog_num_cells(const tos_catalog* c, size_t* n) {
+  if (!c || !n) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  *n = c->cells.size();
+  return TOS_OK;
+}
+
+tos_status tos_catalog_cells(const tos_catalog* c, int64_t* ids, size_t cap) {
+  if (!c || !ids) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (cap < c->cells.size()) return fail(TOS_ERR_INVALID_ARG, "capacity too small");
+  std::copy(c->cells.begin(), c->cells.end(), ids);
+  return TOS_OK;
+}
+
+tos_status tos_catalog_sightline_cells(const tos_catalog* c, int64_t* cells, size_t cap) {
+  if (!c || !cells) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (cap < c->cell_of.size()) return fail(TOS_ERR_INVALID_ARG, "capacity too small");
+  std::copy(c->cell_of.begin(), c->cell_of.end(), cells);
+  return TOS_OK;
+}
+
+tos_status tos_grid_max_angular_scale(const tos_grid* g, double scale, double* max_ang) {
+  TOS_TRY(check_grid(g));
+  if (!max_ang) return fail(TOS_ERR_INVALID_ARG, "max_ang is null");
+  if (g->type != TOS_OBSERVING && !(scale > 0)) return fail(TOS_ERR_INVALID_ARG, "scale must be > 0");
+  *max_ang = max_angular_scale(*g, scale);
+  return TOS_OK;
+}
+
+size_t tos_grid_num_bins(const tos_grid* g) {
+  if (!g || check_grid(g) != TOS_OK) return 0;
+  return (size_t)g->axis[0].nbins * g->axis[1].nbins * g->axis[2].nbins;
+}
+
+void tos_xibin_finalize(tos_xibin* b, size_t n) {
+  // XiBin::finalize (types.h:96-101)
+  for (size_t k = 0; k < n; ++k) {
+    tos_xibin& x = b[k];
+    (x.wgt > 0) ? x.didj /= x.wgt : x.didj = 0;
+    (x.wi > 0) ? x.di /= x.wi : x.di = 0;
+    (x.wj > 0) ? x.dj /= x.wj : x.dj = 0;
+    (x.num_pairs > 0) ? x.z /= (double)x.num_pairs : x.z = 0;
+  }
+}
+
+tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, double scale,
+                      uint32_t flags, tos_xibin* out_bins, tos_xibin* out_cells,
+                      tos_xi_stats* stats) {
+  const auto t_start = std::chrono::steady_clock::now();
+  if (!e || !cat || !out_bins) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (cat->eng != e) return fail(TOS_ERR_INVALID_ARG, "catalogue belongs to another engine");
+  TOS_TRY(check_grid(grid));
+  if ((flags & TOS_XI_SUBSAMPLES) && !out_cells)
+    return fail(TOS_ERR_INVALID_ARG, "TOS_XI_SUBSAMPLES needs out_cells");
+  if (grid->type != TOS_OBSERVING && !(scale > 0 && std::isfinite(scale)))
+    return fail(TOS_ERR_INVALID_ARG, "scale must be a positive finite number");
+  std::lock_guard<std::mutex> lock(e->mu);
+  DeviceGuard dg(e->device);
+  cudaStream_t st = e->stream;
+  const tos_grid& G = *grid;
+  const RefGrid rg = make_ref_grid(G);
+  const uint32_t nb = rg.ntotal;
+  const uint32_t nc = (uint32_t)cat->cells.size();
+  const double max_ang = max_angular_scale(G, scale);
+  const double cos_max = std::cos(max_ang);  // XiEstimator.cc:25
+
+  // --- cell neighbours
+  TOS_TRY(cat->d_nb_count.alloc(nc));
+  TOS_TRY(cat->d_nb_start.alloc(nc + 1));
+  TOS_CUDA_TRY(cudaEventRecord(e->ev[0], st));
+  {
+    const int gb = grid_for(e, nc, 128);
+    k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, nc, max_ang, nullptr, cat->d_nb_count.p,
+                                          nullptr);
+    TOS_CUDA_TRY(cudaGetLastError());
+    std::vector<uint32_t> nbc(nc), nbs(nc + 1, 0);
+    TOS_CUDA_TRY(cudaMemcpyAsync(nbc.data(), cat->d_nb_count.p, nc * 4, cudaMemcpyDeviceToHost, st));
+    TOS_CUDA_TRY(cudaStreamSynchronize(st));
+    for (uint32_t c = 0; c < nc; ++c) nbs[c + 1] = nbs[c] + nbc[c];
+    TOS_TRY(cat->d_nb.alloc(nbs[nc]));
+    TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_nb_start.p, nbs.data(), (nc + 1) * 4,
+                                 cudaMemcpyHostToDevice, st));
+    k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, nc, max_ang, cat->d_nb_start.p, nullptr,
+                                          cat->d_nb.p);
+    TOS_CUDA_TRY(cudaGetLastError());
+  }
+  // --- expansion pass 1: counts
+  const uint32_t nm = (uint32_t)cat->n_los;
+  TOS_TRY(cat->d_cnt.alloc(nm));
+  TOS_TRY(cat->d_cand.alloc(nm));
+  TOS_TRY(cat->d_item_off.alloc(nm));
+  TOS_TRY(cat->d_cell_pairs.alloc(nc));
+  TOS_TRY(cat->d_counters.alloc(4200));
+  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_cell_pairs.p, 0, nc * 8, st));
+  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_counters.p, 0, 4200 * 8, st));
+  unsigned long long* ctr = cat->d_counters.p;  // [0..3] pair kernel, [4] item counter, [8..] sep flags
+  const double theta_min = G.axis[1].min, theta_inv = 1.0 / axis_width(G.axis[1]);
+  const int ge = grid_for(e, (size_t)nm * 32, 256);
+  k_expand<<<ge, 256, 0, st>>>(cat->d_members.p, nm, cat->d_cell_idx.p, cat->d_cell_start.p,
+                               cat->d_nb_start.p, cat->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
+                               cat->d_cnt.p, cat->d_cand.p, cat->d_cell_pairs.p, nullptr, nullptr,
+                               nullptr, nullptr, nullptr, G.type, theta_min, theta_inv, ctr + 8);
+  TOS_CUDA_TRY(cudaGetLastError());
+  // exclusive scan of counts -> item offsets
+  size_t tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cat->d_cnt.p, cat->d_item_off.p, nm, st);
+  TOS_TRY(cat->d_cub_tmp.alloc(tmp_bytes + 16));
+  TOS_CUDA_TRY(cub::DeviceScan::ExclusiveSum(cat->d_cub_tmp.p, tmp_bytes, cat->d_cnt.p,
+                                             cat->d_item_off.p, nm, st));
+  uint32_t last_off = 0, last_cnt = 0;
+  TOS_CUDA_TRY(cudaMemcpyAsync(&last_off, cat->d_item_off.p + nm - 1, 4, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(&last_cnt, cat->d_cnt.p + nm - 1, 4, cudaMemcpyDeviceToHost, st));
+  std::vector<unsigned long long> cell_pairs(nc);
+  TOS_CUDA_TRY(cudaMemcpyAsync(cell_pairs.data(), cat->d_cell_pairs.p, nc * 8,
+                               cudaMemcpyDeviceToHost, st));
+  unsigned long long n_cand_total = 0;
+  {
+    // candidates: reduce on the device
+    size_t tb = 0;
+    cub::DeviceReduce::Sum(nullptr, tb, cat->d_cand.p, ctr + 5, nm, st);
+    if (tb > cat->d_cub_tmp.n) {
+      TOS_CUDA_TRY(cudaStreamSynchronize(st));
+      TOS_TRY(cat->d_cub_tmp.alloc(tb + 16));
+    }
+    TOS_CUDA_TRY(cub::DeviceReduce::Sum(cat->d_cub_tmp.p, tb, cat->d_cand.p, ctr + 5, nm, st));
+    TOS_CUDA_TRY(cudaMemcpyAsync(&n_cand_total, ctr + 5, 8, cudaMemcpyDeviceToHost, st));
+  }
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  const uint64_t n_items = (uint64_t)last_off + last_cnt;
+  unsigned long long n_pixel_pairs = 0, max_cell_pairs = 0;
+  for (auto v : cell_pairs) {
+    n_pixel_pairs += v;
+    max_cell_pairs = std::max(max_cell_pairs, v);
+  }
+  // --- expansion pass 2: items
+  TOS_TRY(cat->d_item_i.alloc(n_items));
+  TOS_TRY(cat->d_item_j.alloc(n_items));
+  TOS_TRY(cat->d_item_c.alloc(n_items));
+  TOS_TRY(cat->d_item_sep.alloc(G.type == TOS_OBSERVING ? n_items : 1));
+  k_expand<<<ge, 256, 0, st>>>(cat->d_members.p, nm, cat->d_cell_idx.p, cat->d_cell_start.p,
+                               cat->d_nb_start.p, cat->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
+                               cat->d_cnt.p, cat->d_cand.p, cat->d_cell_pairs.p, cat->d_item_off.p,
+                               cat->d_item_i.p, cat->d_item_j.p, cat->d_item_c.p,
+                               cat->d_item_sep.p, G.type, theta_min, theta_inv, ctr + 8);
+  TOS_CUDA_TRY(cudaGetLastError());
+  if (G.type == TOS_OBSERVING) {
+    // theta indices within 1e-9 of an edge: recompute with the host libm acos,
+    // the function the reference calls (XiEstimator.cc:166).
+    unsigned long long nflag = 0;
+    TOS_CUDA_TRY(cudaMemcpyAsync(&nflag, ctr + 8, 8, cudaMemcpyDeviceToHost, st));
+    TOS_CUDA_TRY(cudaStreamSynchronize(st));
+    if (nflag > 4096) return fail(TOS_ERR_UNSUPPORTED, "too many theta indices on a bin edge");
+    if (nflag) {
+      std::vector<unsigned long long> at(nflag);
+      TOS_CUDA_TRY(cudaMemcpy(at.data(), ctr + 9, nflag * 8, cudaMemcpyDeviceToHost));
+      for (auto a : at) {
+        double c;
+        TOS_CUDA_TRY(cudaMemcpy(&c, cat->d_item_c.p + a, 8, cudaMemcpyDeviceToHost));
+        const uint32_t sep = tos::ref_u32(tos::dmul(tos::dsub(std::acos(c), theta_min), theta_inv));
+        TOS_CUDA_TRY(cudaMemcpy(cat->d_item_sep.p + a, &sep, 4, cudaMemcpyHostToDevice));
+      }
+    }
+  }
+  TOS_CUDA_TRY(cudaEventRecord(e->ev[1], st));
+
+  // --- accumulation layout and fixed-point scales
+  const size_t acc_words = (size_t)nc * nb * 8;
+  TOS_TRY(cat->d_acc.alloc(acc_words));
+  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_acc.p, 0, acc_words * 8, st));
+  PairArgs A{};
+  A.off = cat->d_off.p;
+  A.npix = cat->d_npix.p;
+  A.dist_pad = cat->d_dist_pad.p;
+  A.loglam_pad = cat->d_loglam_pad.p;
+  A.wd = cat->d_wd.p;
+  A.w = cat->d_w.p;
+  A.prefix = cat->d_prefix.p;
+  A.range = cat->d_range.p;
+  A.cell_idx = cat->d_cell_idx.p;
+  A.item_i = cat->d_item_i.p;
+  A.item_j = cat->d_item_j.p;
+  A.item_c = cat->d_item_c.p;
+  A.item_sep = cat->d_item_sep.p;
+  A.n_items = n_items;
+  A.next_item = ctr + 4;
+  A.g = rg;
+  A.acc = cat->d_acc.p;
+  A.counters = ctr;
+  A.force_exact = (flags & TOS_XI_EXACT) ? 1 : 0;
+  // fixed point: 2^F per field, F = min(window bound, per-cell bound)
+  {
+    const double m = std::max<double>(1.0, cat->max_np);
+    const double wdm = std::max(cat->max_abs_wd, 1e-300), wm = std::max(cat->max_w, 1e-300),
+                 lm = std::max(cat->max_l, 1e-300);
+    const double per_contrib[7] = {wdm * m * wdm, wdm * m, m * wdm, wm * m * wm, wm * m, m * wm,
+                                   lm * m};
+    const double per_pair[7] = {wdm * wdm, wdm, wdm, wm * wm, wm, wm, lm};
+    const double cp = std::max<double>(1.0, (double)max_cell_pairs);
+    for (int k = 0; k < 7; ++k) {
+      const double f1 = 38.0 - std::log2(per_contrib[k]);
+      const double f2 = 62.0 - std::log2(cp * per_pair[k]);
+      int f = (int)std::floor(std::min(f1, f2));
+      f = std::max(-60, std::min(f, 200));
+      A.scale[k] = std::ldexp(1.0, f);
+    }
+  }
+  // FP32 fast-path constants
+  const uint32_t n0 = rg.n0, n1 = (G.type == TOS_OBSERVING) ? 1u : rg.n1;
+  A.inv0f = (float)rg.inv0;
+  A.off0f = (float)(-rg.min0 * rg.inv0);
+  if (G.type == TOS_CARTESIAN) {
+    A.inv1f = 1.0f;
+    A.off1f = (float)(-rg.min1 * rg.inv1);
+    A.inv1sqf = (float)(rg.inv1 * rg.inv1);
+  } else {
+    A.inv1f = (float)rg.inv1;
+    A.off1f = (float)(-rg.min1 * rg.inv1);
+    A.inv1sqf = 1.0f;
+  }
+  A.n0f = (float)n0;
+  A.n1f = (float)n1;
+  A.n0p1f = (float)n0 + 1.0f;
+  A.n1p1f = (float)n1 + 1.0f;
+  A.k0 = std::max(0, std::min(13, 21 - bitlen(n0 + 2)));
+  A.k1 = std::max(0, std::min(13, 21 - bitlen(n1 + 2)));
+  A.mag0 = std::ldexp(1.5f, 23 - A.k0);
+  A.mag1 = std::ldexp(1.5f, 23 - A.k1);
+  std::memcpy(&A.bits0, &A.mag0, 4);
+  std::memcpy(&A.bits1, &A.mag1, 4);
+  A.r2_small = 1e-4f;
+  const bool exact0 = (G.type != TOS_POLAR) && rg.min0 == 0.0 && is_pow2(rg.inv0);
+  const bool minpos = (rg.min0 > 0.0) || (G.type != TOS_OBSERVING && rg.min1 > 0.0) ||
+                      (rg.min0 < 0.0) || (G.type != TOS_OBSERVING && rg.min1 < 0.0);
+  // column pruning window
+  A.prune = cat->sorted ? 1 : 0;
+  {
+    float lim;
+    if (G.type == TOS_POLAR) {
+      // r >= R rejected; r_sq >= s^2 - |float rounding of d1^2| - tiny
+      double R = rg.min0 + (double)n0 / rg.inv0;
+      R = std::max(R, 0.0) * (1.0 + 1e-6) + 1e-6;
+      const double dm = cat->max_d;
+      lim = (float)(std::sqrt(R * R + std::ldexp(dm * dm, -23) + 1e-3) * (1.0 + 1e-6) + 1e-3);
+    } else {
+      lim = first_axis_limit(rg.min0, rg.inv0, n0);
+    }
+    A.win_lim = lim;
+    if (!std::isfinite(lim)) A.prune = 0;
+  }
+  // window layout
+  if (G.type == TOS_CARTESIAN) {
+    A.win_w1 = (int)std::min<uint32_t>(8u, rg.n1);
+    A.win_slots = (int)(n0 * (uint32_t)A.win_w1);
+  } else if (G.type == TOS_POLAR) {
+    A.win_w1 = 0;
+    A.win_slots = (int)std::min<uint32_t>(n0 * rg.n1, 400u);
+  } else {
+    A.win_w1 = 0;
+    A.win_slots = (int)n0;
+  }
+  if ((size_t)A.win_slots * kWinWords * 4 * kPairWarps > 200 * 1024) {
+    // very long first axis: keep only part of it in the window, the rest goes direct
+    A.win_slots = (int)(200 * 1024 / (kWinWords * 4 * kPairWarps));
+    if (G.type == TOS_CARTESIAN) A.win_w1 = std::max(1, A.win_slots / (int)n0);
+    if (G.type == TOS_CARTESIAN && (uint32_t)A.win_w1 * n0 > (uint32_t)A.win_slots) A.win_w1 = 0;
+  }
+  A.contrib_limit = 120;
+  if (cat->max_np > 0) {
+    const uint64_t lim_count = 0xFFFFFFFFull / ((uint64_t)32 * (cat->max_np + 1)) ;
+    if (lim_count < A.contrib_limit) A.contrib_limit = (uint32_t)std::max<uint64_t>(1, lim_count - 1);
+  }
+  if (n_items > 0) {
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    const cudaError_t le =
+        launch_pair_kernel(A, G.type, exact0, minpos, e->num_sms, st);
+    if (le != cudaSuccess) return fail(TOS_ERR_CUDA, std::string("pair kernel: ") + cudaGetErrorString(le));
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[3], st));
+  } else {
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[3], st));
+  }
+  // --- combine cells
+  const bool want_cells = (flags & TOS_XI_SUBSAMPLES) != 0;
+  TOS_TRY(cat->d_out.alloc((size_t)nb * (want_cells ? (size_t)nc + 1 : 1)));
+  double4 ia, ib;
+  ia.x = 1.0 / A.scale[0], ia.y = 1.0 / A.scale[1], ia.z = 1.0 / A.scale[2], ia.w = 1.0 / A.scale[3];
+  ib.x = 1.0 / A.scale[4], ib.y = 1.0 / A.scale[5], ib.z = 1.0 / A.scale[6], ib.w = 0;
+  k_combine<<<grid_for(e, nb, 128), 128, 0, st>>>(cat->d_acc.p, nc, nb, ia, ib, cat->d_out.p,
+                                                   want_cells ? cat->d_out.p + nb : nullptr);
+  TOS_CUDA_TRY(cudaGetLastError());
+  TOS_CUDA_TRY(cudaMemcpyAsync(out_bins, cat->d_out.p, (size_t)nb * sizeof(tos_xibin),
+                               cudaMemcpyDeviceToHost, st));
+  if (want_cells)
+    TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, cat->d_out.p + nb, (size_t)nc * nb * sizeof(tos_xibin),
+                                 cudaMemcpyDeviceToHost, st));
+  unsigned long long hc[4];
+  TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, 32, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->num_sightlines = cat->n_los;
+    stats->num_sightline_pairs = n_cand_total;
+    stats->num_sightline_pairs_used = n_items;
+    stats->num_pixels = cat->n_pix;
+    stats->num_pixel_pairs = n_pixel_pairs;
+    unsigned long long used = 0;
+    for (uint32_t b = 0; b < nb; ++b) used += (unsigned long long)out_bins[b].num_pairs;
+    stats->num_pixel_pairs_used = used + hc[2];
+    stats->num_pixel_pairs_evaluated = hc[0];
+    stats->num_edge_rechecks = hc[1];
+    stats->num_index_overflow = hc[2];
+    stats->num_cells = nc;
+    stats->max_ang = max_ang;
+    stats->cos_max_ang = cos_max;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+    stats->ms_expand = ms;
+    cudaEventElapsedTime(&ms, e->ev[2], e->ev[3]);
+    stats->ms_pairs = ms;
+    cudaEventElapsedTime(&ms, e->ev[0], e->ev[4]);
+    stats->ms_device = ms;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  }
+  return TOS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// engine_internal.h — engine/catalogue objects and helpers shared by the
+// translation units of the pair-counting engine.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tos_common.h"
+
+namespace tos {
+
+// ---- error plumbing -------------------------------------------------------
+void set_error(const std::string& msg);
+tos_status fail(tos_status s, const std::string& msg);
+
+#define TOS_CUDA_TRY(expr)                                                                   \
+  do {                                                                                       \
+    cudaError_t e_ = (expr);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return ::tos::fail(e_ == cudaErrorMemoryAllocation ? TOS_ERR_OOM : TOS_ERR_CUDA,        \
+                         std::string(#expr) + ": " + cudaGetErrorString(e_));               \
+  } while (0)
+
+#define TOS_TRY(expr)                 \
+  do {                                \
+    tos_status s_ = (expr);           \
+    if (s_ != TOS_OK) return s_;      \
+  } while (0)
+
+// Device buffer owned by the engine (freed on destruction / resize).
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  tos_status alloc(size_t count) {
+    if (count <= n && p) return TOS_OK;
+    release();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return fail(TOS_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    }
+    n = count;
+    return TOS_OK;
+  }
+};
+
+}  // namespace tos
+
+struct tos_engine {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  std::mutex mu;
+};
+
+struct tos_catalog {
+  tos_engine* eng = nullptr;
+  size_t n_los = 0, n_pix = 0;
+  int order = 0;
+  int64_t nside = 0;
+  // host-side index
+  std::vector<int64_t> cell_of;     // HEALPix pixel of each sightline
+  std::vector<int64_t> cells;       // occupied cells, ascending
+  std::vector<uint32_t> cell_idx;   // per sightline: index into `cells`
+  std::vector<uint32_t> cell_start; // CSR (n_cells+1) into members
+  std::vector<uint32_t> members;    // sightlines grouped by cell, ascending index within a cell
+  std::vector<uint32_t> npix;       // pixels per sightline
+  std::vector<uint64_t> off;        // compact pixel offset per sightline
+  // device data
+  tos::DevBuf<double4> d_trig;      // sin_dec, cos_dec, sin_ra, cos_ra
+  tos::DevBuf<double4> d_cap;       // cell cap: unit centre xyz, angular radius
+  tos::DevBuf<uint32_t> d_cell_idx, d_cell_start, d_members, d_npix;
+  tos::DevBuf<uint64_t> d_off;      // compact offset (per-pixel double/float arrays)
+  tos::DevBuf<tos_pixel> d_raw;     // uploaded pixels, compact order
+  tos::DevBuf<float> d_dist_pad, d_loglam_pad;
+  tos::DevBuf<double> d_wd;         // w*delta per pixel, exact in double
+  tos::DevBuf<float> d_w;           // weight per pixel
+  tos::DevBuf<double4> d_prefix;    // per sightline N+1 exclusive prefix sums of (w*delta, w, loglam)
+  tos::DevBuf<float4> d_range;      // per sightline (dmin, dmax, lmin, lmax)
+  tos::DevBuf<unsigned int> d_flags;// [0]: 1 if some sightline is not sorted by distance/loglam
+  tos::DevBuf<double> d_maxes;      // [0] max|wd|, [1] max w, [2] max |loglam|, [3] max distance
+  bool sorted = true;
+  double max_abs_wd = 0, max_w = 0, max_l = 0, max_d = 0;
+  uint32_t max_np = 0;
+  // run scratch (kept between runs)
+  tos::DevBuf<uint32_t> d_nb_count, d_nb_start, d_nb;  // cell neighbour CSR
+  tos::DevBuf<uint32_t> d_cnt;                         // per primary: accepted pairs
+  tos::DevBuf<unsigned long long> d_cand;              // per primary candidates (for stats)
+  tos::DevBuf<uint32_t> d_item_off;
+  tos::DevBuf<uint32_t> d_item_i, d_item_j, d_item_sep;
+  tos::DevBuf<double> d_item_c;
+  tos::DevBuf<unsigned long long> d_cell_pairs;        // per cell sum N_i N_j
+  tos::DevBuf<long long> d_acc;                        // [n_cells][n_bins][8] fixed point
+  tos::DevBuf<tos_xibin> d_out;                        // combined / per cell output
+  tos::DevBuf<unsigned long long> d_counters;          // misc counters
+  tos::DevBuf<unsigned char> d_cub_tmp;
+};

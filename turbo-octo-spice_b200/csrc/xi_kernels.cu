@@ -1,0 +1,524 @@
+// xi_kernels.cu — the persistent pixel-pair kernel (see xi_kernels.cuh).
+#include "xi_kernels.cuh"
+
+namespace tos {
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+enum { kPolar = TOS_POLAR, kCart = TOS_CARTESIAN, kObs = TOS_OBSERVING };
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Fixed-point image round(c * scale) of a contribution, |c*scale| < 2^51.
+__device__ __forceinline__ long long to_fixed(double c, double scale) {
+  return __double_as_longlong(__fma_rn(c, scale, kMagic52)) - kMagic52Bits;
+}
+
+// ---- exact re-binning (reference expression order) returning the two axis
+// indices; z is handled per item.  Mirrors ref_bin_* in tos_common.h.
+__device__ __forceinline__ bool exact_cart(float d1, float d2, double c, const RefGrid& g,
+                                           uint32_t* b0, uint32_t* b1) {
+  const double r1_sq = (double)fmul(d1, d1);
+  const double two_r1_cos12 = dmul((double)fmul(2.0f, d1), c);
+  const double r_para = (double)fabsf(fsub(d1, d2));
+  const uint32_t p = ref_u32(dmul(dsub(r_para, g.min0), g.inv0));
+  if (p >= g.n0) return false;
+  const double r_sq = dadd(r1_sq, dmul(dsub((double)d2, two_r1_cos12), (double)d2));
+  const double x = fabs(dsub(r_sq, dmul(r_para, r_para)));
+  const uint32_t q = ref_u32(dmul(dsub(dsqrt(x), g.min1), g.inv1));
+  if (q >= g.n1) return false;
+  *b0 = p;
+  *b1 = q;
+  return true;
+}
+
+__device__ __forceinline__ bool exact_polar(float d1, float d2, double c, const RefGrid& g,
+                                            uint32_t* b0, uint32_t* b1) {
+  const double r1_sq = (double)fmul(d1, d1);
+  const double two_r1_cos12 = dmul((double)fmul(2.0f, d1), c);
+  const double r_sq = dadd(r1_sq, dmul(dsub((double)d2, two_r1_cos12), (double)d2));
+  const double r = dsqrt(r_sq);
+  const uint32_t p = ref_u32(dmul(dsub(r, g.min0), g.inv0));
+  if (p >= g.n0) return false;
+  if (r == 0) return false;
+  const double mu = ddiv((double)fabsf(fsub(d1, d2)), r);
+  const uint32_t q = ref_u32(dmul(dsub(mu, g.min1), g.inv1));
+  if (q >= g.n1) return false;
+  *b0 = p;
+  *b1 = q;
+  return true;
+}
+
+__device__ __forceinline__ bool exact_obs(float l1, float l2, const RefGrid& g, uint32_t* b0) {
+  const uint32_t p = ref_u32(dmul(dsub((double)fabsf(fsub(l1, l2)), g.min0), g.inv0));
+  if (p >= g.n0) return false;
+  *b0 = p;
+  return true;
+}
+
+__device__ __forceinline__ uint32_t zbin_of_sum(float lsum, const RefGrid& g) {
+  return ref_u32(dmul(dsub(dmul(0.5, (double)lsum), g.min2), g.invn2));
+}
+
+// Per-row (lane) state of a chunk.
+struct Row {
+  float x1;     // distance (or loglam for observing coordinates)
+  float d1, l1; // raw distance and loglam for the exact path
+  float A1;     // Cartesian: d1 * a * inv1^2; Polar: d1 * a
+  float dl1;    // float rounding of d1*d1 (scaled like A1), exact residual
+  double wd1, w1, hl1;  // w*delta, w, 0.5*loglam
+};
+
+// Per-item constants shared by the warp.
+struct Item {
+  uint32_t i, j, ni, nj, cell;
+  double c;
+  float ap;          // 2(1-c) [* inv1^2 for Cartesian]
+  uint32_t zb;       // constant z index of the item
+  uint32_t sep;      // observing: theta index
+  int zconst;        // z index constant over the item
+  int lo1;           // Cartesian window: first axis-1 bin
+  const float* colx; // padded column coordinate (distance or loglam) of sightline j
+  const float* coll; // padded column loglam
+  const float* cold; // padded column distance
+  const double4* pre;// prefix sums of sightline j
+};
+
+// Window slot of a packed key (b0 << 16 | b1), or -1 when outside the window.
+template <int COORD>
+__device__ __forceinline__ int window_slot(const PairArgs& A, const Item& it, uint32_t key) {
+  const int b0 = (int)(key >> 16), b1 = (int)(key & 0xFFFFu);
+  if (COORD == kCart) {
+    const int d = b1 - it.lo1;
+    return (d >= 0 && d < A.win_w1) ? b0 * A.win_w1 + d : -1;
+  } else if (COORD == kPolar) {
+    return (A.g.n0 * A.g.n1 <= (uint32_t)A.win_slots) ? b0 * (int)A.g.n1 + b1 : -1;
+  } else {
+    return (b0 < A.win_slots) ? b0 : -1;
+  }
+}
+
+// Flat reference index of a packed key with the item's z index (unsigned
+// arithmetic as in XiEstimator.cc:196-201, 249-254, 283-288).
+template <int COORD>
+__device__ __forceinline__ uint32_t flat_index(const PairArgs& A, const Item& it, uint32_t key) {
+  const uint32_t b0 = key >> 16, b1 = key & 0xFFFFu;
+  uint32_t b = (COORD == kObs) ? it.sep + b0 * A.g.n1 : b1 + b0 * A.g.n1;
+  return it.zb + b * A.g.n2;
+}
+
+// Add one run's contribution directly to the global per-cell accumulator.
+__device__ __forceinline__ void add_direct(const PairArgs& A, uint32_t cell, uint32_t idx,
+                                           const double* c, uint32_t m) {
+  if (idx >= A.g.ntotal) {
+    atomicAdd(&A.counters[2], (unsigned long long)m);
+    return;
+  }
+  unsigned long long* base =
+      (unsigned long long*)(A.acc + ((size_t)cell * A.g.ntotal + idx) * 8);
+#pragma unroll
+  for (int k = 0; k < 7; ++k) atomicAdd(base + k, (unsigned long long)to_fixed(c[k], A.scale[k]));
+  atomicAdd(base + 7, (unsigned long long)m);
+  atomicAdd(&A.counters[3], 1ull);
+}
+
+// Move the warp window into the global accumulators and clear it.
+template <int COORD>
+__device__ void flush_window(const PairArgs& A, const Item& it, uint32_t* win, int lane) {
+  const int S = A.win_slots;
+  int nslots = (COORD == kCart) ? (int)A.g.n0 * A.win_w1
+               : (COORD == kPolar) ? (int)(A.g.n0 * A.g.n1)
+                                   : (int)A.g.n0;
+  if (nslots > S) nslots = S;
+  for (int s = lane; s < nslots; s += 32) {
+    const uint32_t cnt = win[14 * S + s];
+    if (cnt == 0) continue;
+    uint32_t key;
+    if (COORD == kCart)
+      key = ((uint32_t)(s / A.win_w1) << 16) | (uint32_t)(it.lo1 + s % A.win_w1);
+    else if (COORD == kPolar)
+      key = ((uint32_t)(s / (int)A.g.n1) << 16) | (uint32_t)(s % (int)A.g.n1);
+    else
+      key = (uint32_t)s << 16;
+    const uint32_t idx = flat_index<COORD>(A, it, key);
+    if (idx < A.g.ntotal) {
+      unsigned long long* base =
+          (unsigned long long*)(A.acc + ((size_t)it.cell * A.g.ntotal + idx) * 8);
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+        const uint32_t lo = win[(2 * k) * S + s];
+        const int hi = (int)win[(2 * k + 1) * S + s];
+        const long long q = ((long long)hi << kSplit) + (long long)lo;
+        atomicAdd(base + k, (unsigned long long)q);
+      }
+      atomicAdd(base + 7, (unsigned long long)cnt);
+    } else {
+      atomicAdd(&A.counters[2], (unsigned long long)cnt);
+    }
+#pragma unroll
+    for (int w = 0; w < kWinWords; ++w) win[w * S + s] = 0u;
+  }
+  __syncwarp();
+}
+
+// FP32 binning of one pixel pair.  key = packed (b0, b1) or kInvalidKey;
+// recheck = the pair lies within 2^-K bins of a decision edge (or in a
+// degenerate corner) and must be re-binned in FP64.
+template <int COORD, bool EXACT0, bool MINPOS>
+__device__ __forceinline__ void fast_bin(const PairArgs& A, const Row& R, float x2, uint32_t& key,
+                                         bool& recheck) {
+  float t0, t1;
+  bool small = false;
+  if (COORD == kCart) {
+    const float s = __fsub_rn(x2, R.x1);
+    t0 = __fmaf_rn(fabsf(s), A.inv0f, A.off0f);
+    const float u = fabsf(__fmaf_rn(R.A1, x2, R.dl1));
+    t1 = __fadd_rn(sqrt_approx(u), A.off1f);
+  } else if (COORD == kPolar) {
+    const float s = __fsub_rn(x2, R.x1);
+    const float r2 = __fmaf_rn(s, s, __fmaf_rn(R.A1, x2, R.dl1));
+    const float rs = rsqrt_approx(r2);
+    t0 = __fmaf_rn(__fmul_rn(r2, rs), A.inv0f, A.off0f);
+    t1 = __fmaf_rn(__fmul_rn(fabsf(s), rs), A.inv1f, A.off1f);
+    small = !(r2 >= A.r2_small);
+  } else {
+    const float dl = fabsf(__fsub_rn(x2, R.x1));
+    t0 = __fmaf_rn(dl, A.inv0f, A.off0f);
+    t1 = 0.5f;
+  }
+  const int q0 = __float_as_int(__fadd_rz(t0, A.mag0)) - A.bits0;
+  const int q1 = __float_as_int(__fadd_rz(t1, A.mag1)) - A.bits1;
+  bool valid = (t0 < A.n0f) && (t1 < A.n1f);
+  bool coarse = (t0 < A.n0p1f) && (t1 < A.n1p1f);
+  if (MINPOS) {
+    valid = valid && (t0 > -1.0f) && (t1 > -1.0f);
+    coarse = coarse && (t0 > -2.0f) && (t1 > -2.0f);
+  }
+  int b0 = q0 >> A.k0, b1 = q1 >> A.k1;
+  if (MINPOS) {
+    b0 = max(b0, 0);
+    b1 = max(b1, 0);
+  }
+  key = valid ? (((uint32_t)b0 << 16) | (uint32_t)b1) : kInvalidKey;
+  bool edge = (((q1 + 1) & ((1 << A.k1) - 1)) < 2);
+  if (COORD == kObs) edge = false;
+  if (!EXACT0) edge = edge || (((q0 + 1) & ((1 << A.k0) - 1)) < 2);
+  recheck = (coarse && edge) || small;
+}
+
+// Exact (FP64 reference) key of one pair.
+template <int COORD>
+__device__ __forceinline__ uint32_t exact_key(const PairArgs& A, const Row& R, const Item& it,
+                                              float x2, float d2) {
+  uint32_t b0 = 0, b1 = 0;
+  bool ok;
+  if (COORD == kCart)
+    ok = exact_cart(R.d1, d2, it.c, A.g, &b0, &b1);
+  else if (COORD == kPolar)
+    ok = exact_polar(R.d1, d2, it.c, A.g, &b0, &b1);
+  else
+    ok = exact_obs(R.x1, x2, A.g, &b0);
+  return ok ? ((b0 << 16) | b1) : kInvalidKey;
+}
+
+// Exact flat key including a per-pair z index (items whose z index varies).
+template <int COORD>
+__device__ __forceinline__ uint32_t exact_flat_key(const PairArgs& A, const Row& R, const Item& it,
+                                                   float x2, float d2, float l2) {
+  uint32_t idx = 0;
+  bool ok;
+  if (COORD == kCart)
+    ok = ref_bin_cartesian(R.d1, R.l1, d2, l2, it.c, A.g, &idx);
+  else if (COORD == kPolar)
+    ok = ref_bin_polar(R.d1, R.l1, d2, l2, it.c, A.g, &idx);
+  else
+    ok = ref_bin_observing(R.l1, l2, it.sep, A.g, &idx);
+  // kInvalidKey is reserved; an index equal to it can only be an overflow.
+  return ok ? (idx == kInvalidKey ? kInvalidKey - 1u : idx) : kInvalidKey;
+}
+
+// Sweep one 32-row chunk.  MODE 0: fast path with packed keys and the warp
+// window; MODE 1: every pair exact, flat keys, direct global adds.
+template <int COORD, bool EXACT0, bool MINPOS, int MODE>
+__device__ void sweep_chunk(const PairArgs& A, const Item& it, const Row& R, bool active,
+                            int t_begin, int t_end, uint32_t* win, int lane,
+                            unsigned long long& n_recheck, uint32_t& ncontrib) {
+  uint32_t cur = kInvalidKey;
+  int run_start = 0;
+  double ps0 = 0, ps1 = 0, ps2 = 0;
+
+  auto close_run = [&](int p_end, const double4& pn) {
+    const uint32_t m = (uint32_t)(p_end - run_start);
+    const double md = (double)m;
+    const double dwd = pn.x - ps0, dw = pn.y - ps1, dl = pn.z - ps2;
+    double c[7];
+    c[0] = R.wd1 * dwd;
+    c[1] = R.wd1 * md;
+    c[2] = dwd;
+    c[3] = R.w1 * dw;
+    c[4] = R.w1 * md;
+    c[5] = dw;
+    c[6] = __fma_rn(R.hl1, md, 0.5 * dl);
+    if (MODE == 0) {
+      const int slot = window_slot<COORD>(A, it, cur);
+      if (slot >= 0) {
+        const int S = A.win_slots;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+          const long long q = to_fixed(c[k], A.scale[k]);
+          atomicAdd(&win[(2 * k) * S + slot], (uint32_t)q & ((1u << kSplit) - 1u));
+          atomicAdd(&win[(2 * k + 1) * S + slot], (uint32_t)(int)(q >> kSplit));
+        }
+        atomicAdd(&win[14 * S + slot], m);
+        ++ncontrib;
+      } else {
+        add_direct(A, it.cell, flat_index<COORD>(A, it, cur), c, m);
+      }
+    } else {
+      add_direct(A, it.cell, cur, c, m);
+    }
+  };
+
+  for (int t = t_begin; t < t_end; ++t) {
+    const int p2 = t + lane;
+    const float x2 = it.colx[p2];
+    uint32_t key;
+    bool recheck;
+    if (MODE == 0) {
+      fast_bin<COORD, EXACT0, MINPOS>(A, R, x2, key, recheck);
+      if (__any_sync(kFull, recheck)) {
+        if (recheck) {
+          key = exact_key<COORD>(A, R, it, x2, (COORD == kObs) ? 0.f : x2);
+          ++n_recheck;
+        }
+      }
+    } else {
+      key = kInvalidKey;
+      if (active && p2 >= 0 && p2 < (int)it.nj) {
+        const float d2 = it.cold[p2], l2 = it.coll[p2];
+        key = exact_flat_key<COORD>(A, R, it, x2, d2, l2);
+      }
+    }
+    const bool changed = key != cur;
+    if (__any_sync(kFull, changed)) {
+      if (changed) {
+        const int pc = min(max(p2, 0), (int)it.nj);
+        const double4 pn = it.pre[pc];
+        if (cur != kInvalidKey) close_run(p2, pn);
+        cur = key;
+        run_start = p2;
+        ps0 = pn.x;
+        ps1 = pn.y;
+        ps2 = pn.z;
+      }
+      if (MODE == 0 && __any_sync(kFull, ncontrib >= A.contrib_limit)) {
+        flush_window<COORD>(A, it, win, lane);
+        ncontrib = 0;
+      }
+    }
+  }
+  // close runs still open at the end of the sweep
+  if (cur != kInvalidKey) {
+    const int p_end = t_end + lane;
+    const int pc = min(max(p_end, 0), (int)it.nj);
+    close_run(p_end, it.pre[pc]);
+  }
+}
+
+// Lower bound on the sorted padded column array: first p in [0, n) with
+// pred(x[p]) true, pred monotone (false ... false true ... true).
+template <class Pred>
+__device__ __forceinline__ int lower_bound_pred(const float* x, int n, Pred pred) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (pred(x[mid]))
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
+template <int COORD, bool EXACT0, bool MINPOS, int MODE>
+__device__ void process_item(const PairArgs& A, Item& it, uint32_t* win, int lane,
+                             unsigned long long& n_eval, unsigned long long& n_recheck) {
+  const uint64_t oi = A.off[it.i];
+  const float* rowd = A.dist_pad + oi + (uint64_t)kPad * (it.i + 1);
+  const float* rowl = A.loglam_pad + oi + (uint64_t)kPad * (it.i + 1);
+  const double* rowwd = A.wd + oi;
+  const float* roww = A.w + oi;
+  uint32_t ncontrib = 0;  // window contributions of this lane since the last flush
+  for (uint32_t r0 = 0; r0 < it.ni; r0 += 32) {
+    const uint32_t row = r0 + lane;
+    const bool active = row < it.ni;
+    Row R;
+    if (active) {
+      R.d1 = rowd[row];
+      R.l1 = rowl[row];
+      R.wd1 = rowwd[row];
+      R.w1 = (double)roww[row];
+      R.hl1 = 0.5 * (double)R.l1;
+      R.x1 = (COORD == kObs) ? R.l1 : R.d1;
+      const float p = __fmul_rn(R.d1, R.d1);
+      const float e = __fmaf_rn(R.d1, R.d1, -p);  // d1*d1 = p + e exactly
+      if (COORD == kCart) {
+        R.A1 = __fmul_rn(R.d1, it.ap);
+        R.dl1 = __fmul_rn(-e, A.inv1sqf);
+      } else if (COORD == kPolar) {
+        R.A1 = __fmul_rn(R.d1, it.ap);
+        R.dl1 = -e;
+      } else {
+        R.A1 = 0.f;
+        R.dl1 = 0.f;
+      }
+    } else {
+      R.d1 = R.l1 = 0.f;
+      R.wd1 = R.w1 = R.hl1 = 0.0;
+      R.x1 = -kSentinel;
+      R.A1 = 0.f;
+      R.dl1 = 0.f;
+    }
+    // column window of this chunk
+    int t_begin, t_end;
+    if (A.prune) {
+      int lo = (int)it.nj, hi = 0;
+      if (active) {
+        const float x1 = R.x1, lim = A.win_lim;
+        lo = lower_bound_pred(it.colx, (int)it.nj, [&](float x2) { return __fsub_rn(x1, x2) < lim; });
+        hi = lower_bound_pred(it.colx, (int)it.nj,
+                              [&](float x2) { return x2 >= x1 && __fsub_rn(x2, x1) >= lim; });
+      }
+      int tb = active ? lo - lane : 0x7FFFFFFF;
+      int te = active ? hi - lane : -0x7FFFFFFF;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        tb = min(tb, __shfl_xor_sync(kFull, tb, o));
+        te = max(te, __shfl_xor_sync(kFull, te, o));
+      }
+      t_begin = tb;
+      t_end = te;
+    } else {
+      t_begin = -31;
+      t_end = (int)it.nj;
+    }
+    if (t_end <= t_begin) continue;
+    if (active) {
+      const int a = max(t_begin + (int)lane, 0), b = min(t_end + (int)lane, (int)it.nj);
+      if (b > a) n_eval += (unsigned long long)(b - a);
+    }
+    sweep_chunk<COORD, EXACT0, MINPOS, MODE>(A, it, R, active, t_begin, t_end, win, lane,
+                                            n_recheck, ncontrib);
+  }
+  if (MODE == 0) flush_window<COORD>(A, it, win, lane);
+}
+
+template <int COORD, bool EXACT0, bool MINPOS>
+__global__ void __launch_bounds__(kPairWarps * 32, 1) pair_kernel(PairArgs A) {
+  extern __shared__ uint32_t smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* win = smem + (size_t)warp * kWinWords * A.win_slots;
+  for (int k = lane; k < kWinWords * A.win_slots; k += 32) win[k] = 0u;
+  __syncwarp();
+  unsigned long long n_eval = 0, n_recheck = 0;
+  for (;;) {
+    unsigned long long idx = 0;
+    if (lane == 0) idx = atomicAdd(A.next_item, 1ull);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= A.n_items) break;
+    Item it;
+    it.i = A.item_i[idx];
+    it.j = A.item_j[idx];
+    it.c = A.item_c[idx];
+    it.ni = A.npix[it.i];
+    it.nj = A.npix[it.j];
+    if (it.ni == 0 || it.nj == 0) continue;
+    it.cell = A.cell_idx[it.i];
+    it.sep = (COORD == kObs) ? A.item_sep[idx] : 0u;
+    const uint64_t oj = A.off[it.j] + (uint64_t)kPad * (it.j + 1);
+    it.cold = A.dist_pad + oj;
+    it.coll = A.loglam_pad + oj;
+    it.colx = (COORD == kObs) ? it.coll : it.cold;
+    it.pre = A.prefix + A.off[it.j] + it.j;
+    const double a = 2.0 * dsub(1.0, it.c);
+    it.ap = (COORD == kCart) ? (float)(a * A.g.inv1 * A.g.inv1) : (float)a;
+    // z index: constant over the item when both ends of the loglam-sum range agree
+    const float4 ri = A.range[it.i], rj = A.range[it.j];
+    const float lsum_lo = __fadd_rn(ri.z, rj.z), lsum_hi = __fadd_rn(ri.w, rj.w);
+    const double zlo = dmul(dsub(dmul(0.5, (double)lsum_lo), A.g.min2), A.g.invn2);
+    const double zhi = dmul(dsub(dmul(0.5, (double)lsum_hi), A.g.min2), A.g.invn2);
+    it.zb = zbin_of_sum(lsum_lo, A.g);
+    it.zconst = (zlo > -1.0 && zhi < 2147483648.0 && it.zb == zbin_of_sum(lsum_hi, A.g)) ? 1 : 0;
+    // Cartesian window along axis 1 from the distance ranges
+    it.lo1 = 0;
+    if (COORD == kCart) {
+      const float ulo = it.ap * ri.x * rj.x, uhi = it.ap * ri.y * rj.y;
+      const float slack = 1e-3f + 2e-7f * (ri.y * ri.y) * A.inv1sqf;
+      const float tlo = sqrtf(fmaxf(ulo * (1.f - 1e-5f) - slack, 0.f)) + A.off1f;
+      int lo1 = (int)floorf(tlo - 1e-2f);
+      it.lo1 = max(0, min(lo1, (int)A.g.n1 - 1));
+      (void)uhi;
+    }
+    const bool exact_item = A.force_exact || !it.zconst;
+    if (exact_item)
+      process_item<COORD, EXACT0, MINPOS, 1>(A, it, win, lane, n_eval, n_recheck);
+    else
+      process_item<COORD, EXACT0, MINPOS, 0>(A, it, win, lane, n_eval, n_recheck);
+  }
+  // counters
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_eval += __shfl_xor_sync(kFull, n_eval, o);
+    n_recheck += __shfl_xor_sync(kFull, n_recheck, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&A.counters[0], n_eval);
+    atomicAdd(&A.counters[1], n_recheck);
+  }
+}
+
+template <int COORD, bool EXACT0, bool MINPOS>
+cudaError_t launch3(const PairArgs& a, int grid, cudaStream_t stream) {
+  const size_t smem = pair_kernel_smem(a.win_slots);
+  auto k = pair_kernel<COORD, EXACT0, MINPOS>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, kPairWarps * 32, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <int COORD>
+cudaError_t launch2(const PairArgs& a, bool exact0, bool minpos, int grid, cudaStream_t stream) {
+  if (exact0)
+    return minpos ? launch3<COORD, true, true>(a, grid, stream)
+                  : launch3<COORD, true, false>(a, grid, stream);
+  return minpos ? launch3<COORD, false, true>(a, grid, stream)
+                : launch3<COORD, false, false>(a, grid, stream);
+}
+
+}  // namespace
+
+size_t pair_kernel_smem(int win_slots) {
+  return (size_t)kPairWarps * kWinWords * (size_t)win_slots * sizeof(uint32_t);
+}
+
+cudaError_t launch_pair_kernel(const PairArgs& a, int coord, bool exact0, bool minpos, int grid,
+                               cudaStream_t stream) {
+  switch (coord) {
+    case TOS_CARTESIAN: return launch2<kCart>(a, exact0, minpos, grid, stream);
+    case TOS_POLAR: return launch2<kPolar>(a, exact0, minpos, grid, stream);
+    default: return launch2<kObs>(a, exact0, minpos, grid, stream);
+  }
+}
+
+}  // namespace tos

@@ -1,0 +1,85 @@
+// xi_kernels.cuh — device code of the XiEstimator pair count.
+//
+// Work decomposition (replaces XiEstimator::run's one-task-per-sky-cell
+// ThreadPool loop, XiEstimator.cc:31-44 and 121-159):
+//   1. a work item is one accepted sightline pair (i, j), i < j,
+//      cos(theta_ij) > cos(max_ang), attributed to the cell of i;
+//   2. persistent warps pull work items from a global counter; a warp sweeps
+//      the N_i x N_j pixel-pair matrix of its item in chunks of 32 rows
+//      (lane = row p1 of sightline i) along skewed diagonals: at step t lane L
+//      looks at column p2 = t + L of sightline j, so all lanes see the same
+//      line-of-sight separation at the same step and change bins together;
+//   3. every pair is binned in FP32 (well-conditioned forms of the reference's
+//      expressions); pairs within 2^-K bins of an edge are re-binned with the
+//      reference's exact FP64 expression order;
+//   4. each lane keeps a run of consecutive columns with the same bin; when the
+//      bin changes, the run's contribution to all eight XiBin fields comes
+//      from FP64 prefix sums of sightline j, is quantised to 64-bit fixed point
+//      and added with two u32 shared-memory atomics per field into the warp's
+//      private window (u32 adds are native; aligned lanes hit the same slot
+//      and are combined by the hardware);
+//   5. at the end of the item the window is added into per-cell int64
+//      accumulators in global memory, so every sum is exact, deterministic
+//      and independent of scheduling.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "tos_common.h"
+
+namespace tos {
+
+constexpr uint32_t kInvalidKey = 0xFFFFFFFFu;
+constexpr int kPairWarps = 8;   // warps per CTA of the pair kernel
+constexpr int kWinWords = 15;   // u32 words per window slot: 7 x (lo, hi) + count
+constexpr int kSplit = 20;      // bits in the low word of the fixed-point split
+constexpr double kMagic52 = 6755399441055744.0;  // 1.5 * 2^52
+constexpr long long kMagic52Bits = 0x4338000000000000LL;
+
+struct PairArgs {
+  // catalogue
+  const uint64_t* off;       // compact pixel offset of each sightline
+  const uint32_t* npix;      // pixels per sightline
+  const float* dist_pad;     // padded distances
+  const float* loglam_pad;   // padded log10 wavelengths
+  const double* wd;          // w * delta (exact double) per pixel
+  const float* w;            // weight per pixel
+  const double4* prefix;     // per sightline, N+1 exclusive prefix sums of (wd, w, loglam)
+  const float4* range;       // per sightline (dmin, dmax, lmin, lmax)
+  const uint32_t* cell_idx;  // cell index of each sightline
+  // work items
+  const uint32_t* item_i;
+  const uint32_t* item_j;
+  const double* item_c;
+  const uint32_t* item_sep;  // theta index (observing coordinates)
+  unsigned long long n_items;
+  unsigned long long* next_item;
+  // grid (reference constants and FP32 fast-path maps t = x * inv + off)
+  RefGrid g;
+  float inv0f, off0f, inv1f, off1f;
+  float n0f, n1f, n0p1f, n1p1f;
+  float inv1sqf;             // Cartesian: u = X * inv1^2
+  float mag0, mag1;          // 1.5 * 2^(23-K) for the two axes
+  int k0, k1;                // fractional bits kept (edge half-width 2^-K)
+  int bits0, bits1;          // bit patterns of mag0/mag1
+  float r2_small;            // Polar: squared separations below this are re-binned in FP64
+  float win_lim;             // |x1 - x2| >= win_lim (float) is always rejected
+  int prune;                 // sightlines sorted: restrict columns to the r_par window
+  // accumulation
+  double scale[7];           // 2^F per field
+  int win_w1;                // window width along axis 1 (Cartesian)
+  int win_slots;             // slots per warp window
+  uint32_t contrib_limit;    // contributions per lane before a window flush
+  long long* acc;            // [n_cells][ntotal][8] fixed point
+  unsigned long long* counters;  // [0] evaluated pairs [1] rechecks [2] overflow pairs [3] direct runs
+  int force_exact;           // evaluate every pixel pair with the FP64 reference
+};
+
+// Launch the persistent pair kernel (coordinate type from a.g/a.* fields).
+cudaError_t launch_pair_kernel(const PairArgs& a, int coord, bool exact0, bool minpos, int grid,
+                               cudaStream_t stream);
+size_t pair_kernel_smem(int win_slots);
+
+}  // namespace tos

@@ -1,0 +1,284 @@
+"""Python bindings of the B200 pair-counting engine (ctypes over include/tos_b200.h).
+
+The engine is the in-tree shared library ``lib/libtos_b200.so`` built by the
+package Makefile.  There is no Python or CPU implementation of the hot path
+here: every compute call goes through the library, and loading fails loudly
+when it has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libtos_b200.so")
+
+TOS_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA", 4: "TIMEOUT", 5: "UNSUPPORTED",
+                6: "NO_DEVICE", 7: "INTERNAL"}
+POLAR, CARTESIAN, OBSERVING = 0, 1, 2
+XI_SUBSAMPLES = 0x1
+XI_EXACT = 0x2
+
+# numpy views of the C structs
+PIXEL_DTYPE = np.dtype([("value", "<f4"), ("loglam", "<f4"), ("weight", "<f4"), ("distance", "<f4")])
+SIGHTLINE_DTYPE = np.dtype([("ra", "<f8"), ("dec", "<f8"), ("forest_id", "<i4"), ("plate", "<i4"),
+                            ("pixel_offset", "<u8"), ("num_pixels", "<u4"), ("reserved", "<u4")])
+XIBIN_DTYPE = np.dtype([("didj", "<f8"), ("di", "<f8"), ("dj", "<f8"), ("wgt", "<f8"), ("wi", "<f8"),
+                        ("wj", "<f8"), ("z", "<f8"), ("num_pairs", "<i8")])
+
+
+class TosError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class _Axis(C.Structure):
+    _fields_ = [("min", C.c_double), ("max", C.c_double), ("nbins", C.c_int32), ("reserved", C.c_int32)]
+
+
+class _Grid(C.Structure):
+    _fields_ = [("type", C.c_int32), ("reserved", C.c_int32), ("axis", _Axis * 3)]
+
+
+class XiStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "num_sightlines", "num_sightline_pairs", "num_sightline_pairs_used", "num_pixels",
+        "num_pixel_pairs", "num_pixel_pairs_used", "num_pixel_pairs_evaluated", "num_edge_rechecks",
+        "num_index_overflow", "num_cells")] + [(n, C.c_double) for n in (
+            "max_ang", "cos_max_ang", "ms_expand", "ms_pairs", "ms_total", "ms_device")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The engine library (loaded once). Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"engine library not built: {LIB_PATH} (run make in {PKG_ROOT})")
+        L = C.CDLL(LIB_PATH)
+        vp, sz, i32, u32, dbl = C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_double
+        L.tos_last_error.restype = C.c_char_p
+        L.tos_abi_version.restype = C.c_int
+        L.tos_engine_create.argtypes = [i32, C.POINTER(vp)]
+        L.tos_engine_destroy.argtypes = [vp]
+        L.tos_engine_destroy.restype = None
+        L.tos_catalog_create.argtypes = [vp, vp, sz, vp, sz, i32, C.POINTER(vp)]
+        L.tos_catalog_destroy.argtypes = [vp]
+        L.tos_catalog_destroy.restype = None
+        L.tos_catalog_num_cells.argtypes = [vp, C.POINTER(sz)]
+        L.tos_catalog_cells.argtypes = [vp, vp, sz]
+        L.tos_catalog_sightline_cells.argtypes = [vp, vp, sz]
+        L.tos_grid_max_angular_scale.argtypes = [C.POINTER(_Grid), dbl, C.POINTER(dbl)]
+        L.tos_grid_num_bins.argtypes = [C.POINTER(_Grid)]
+        L.tos_grid_num_bins.restype = sz
+        L.tos_xi_run.argtypes = [vp, vp, C.POINTER(_Grid), dbl, u32, vp, vp, C.POINTER(XiStats)]
+        L.tos_xibin_finalize.argtypes = [vp, sz]
+        L.tos_xibin_finalize.restype = None
+        L.tos_brute_run.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
+        L.tos_comoving_distance.argtypes = [dbl, vp, sz, vp]
+        L.tos_fill_distances.argtypes = [dbl, vp, sz]
+        for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
+                     "tos_catalog_sightline_cells", "tos_grid_max_angular_scale", "tos_xi_run",
+                     "tos_brute_run", "tos_comoving_distance", "tos_fill_distances"):
+            getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _check(status: int):
+    if status != TOS_OK:
+        raise TosError(status, lib().tos_last_error().decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass(frozen=True)
+class Axis:
+    """Linear axis "[min:max]*nbins" (likely's uniform binning)."""
+    min: float
+    max: float
+    nbins: int
+
+    @staticmethod
+    def parse(spec: str) -> "Axis":
+        s = spec.strip()
+        if not (s.startswith("[") and "]*" in s and ":" in s):
+            raise ValueError(f"bad binning specification: {spec}")
+        rng, n = s[1:].split("]*")
+        lo, hi = rng.split(":")
+        return Axis(float(lo), float(hi), int(n))
+
+    @property
+    def width(self) -> float:
+        return (self.max - self.min) / self.nbins
+
+
+@dataclass(frozen=True)
+class Grid:
+    """A three-axis binning grid with its coordinate type (AbsTwoPointGrid + subclass)."""
+    type: int
+    axes: tuple
+
+    @staticmethod
+    def cartesian(rpar="[0:200]*50", rperp="[0:200]*50", z="[3.556:3.735]*1") -> "Grid":
+        return Grid(CARTESIAN, tuple(Axis.parse(a) for a in (rpar, rperp, z)))
+
+    @staticmethod
+    def polar(r="[0:200]*50", mu="[0:1]*20", z="[3.556:3.735]*1") -> "Grid":
+        return Grid(POLAR, tuple(Axis.parse(a) for a in (r, mu, z)))
+
+    @staticmethod
+    def observing(dloglam="[0:0.05]*25", theta="[5:175]*1", z="[3.556:3.735]*1") -> "Grid":
+        return Grid(OBSERVING, tuple(Axis.parse(a) for a in (dloglam, theta, z)))
+
+    def c_struct(self) -> _Grid:
+        g = _Grid()
+        g.type = self.type
+        for k, a in enumerate(self.axes):
+            g.axis[k].min, g.axis[k].max, g.axis[k].nbins = a.min, a.max, a.nbins
+        return g
+
+    @property
+    def nbins(self) -> int:
+        return int(self.axes[0].nbins * self.axes[1].nbins * self.axes[2].nbins)
+
+    def axes_array(self) -> np.ndarray:
+        return np.array([[a.min, a.max, a.nbins] for a in self.axes], dtype=np.float64).ravel()
+
+    def max_angular_scale(self, scale: float) -> float:
+        out = C.c_double()
+        _check(lib().tos_grid_max_angular_scale(C.byref(self.c_struct()), scale, C.byref(out)))
+        return out.value
+
+
+class Engine:
+    """A CUDA device owned by the engine (tos_engine)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().tos_engine_create(device, C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tos_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Catalog:
+    """Sightlines and pixels resident on the device, binned into HEALPix cells."""
+
+    def __init__(self, engine: Engine, sightlines: np.ndarray, pixels: np.ndarray, healpix_order: int):
+        sightlines = np.ascontiguousarray(sightlines, dtype=SIGHTLINE_DTYPE)
+        pixels = np.ascontiguousarray(pixels, dtype=PIXEL_DTYPE)
+        h = C.c_void_p()
+        _check(lib().tos_catalog_create(engine.handle, _ptr(sightlines), len(sightlines), _ptr(pixels),
+                                        len(pixels), healpix_order, C.byref(h)))
+        self._h = h
+        self.engine = engine
+        self.n_sightlines = len(sightlines)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def num_cells(self) -> int:
+        n = C.c_size_t()
+        _check(lib().tos_catalog_num_cells(self._h, C.byref(n)))
+        return n.value
+
+    def cells(self) -> np.ndarray:
+        n = self.num_cells()
+        out = np.zeros(n, dtype=np.int64)
+        _check(lib().tos_catalog_cells(self._h, _ptr(out), n))
+        return out
+
+    def sightline_cells(self) -> np.ndarray:
+        out = np.zeros(self.n_sightlines, dtype=np.int64)
+        _check(lib().tos_catalog_sightline_cells(self._h, _ptr(out), self.n_sightlines))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tos_catalog_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def xi_run(engine: Engine, catalog: Catalog, grid: Grid, scale: float, subsamples: bool = False,
+           exact: bool = False):
+    """Pair count of XiEstimator::run. Returns (bins, cells or None, stats dict);
+    bins/cells are raw (unfinalized) XiBin sums as XIBIN_DTYPE arrays."""
+    nb = grid.nbins
+    bins = np.zeros(nb, dtype=XIBIN_DTYPE)
+    cells = np.zeros((catalog.num_cells(), nb), dtype=XIBIN_DTYPE) if subsamples else None
+    flags = (XI_SUBSAMPLES if subsamples else 0) | (XI_EXACT if exact else 0)
+    st = XiStats()
+    _check(lib().tos_xi_run(engine.handle, catalog.handle, C.byref(grid.c_struct()), scale, flags, _ptr(bins),
+                            _ptr(cells) if cells is not None else None, C.byref(st)))
+    return bins, cells, st.as_dict()
+
+
+def finalize(bins: np.ndarray) -> np.ndarray:
+    """XiBin::finalize on a copy."""
+    out = np.ascontiguousarray(bins.copy(), dtype=XIBIN_DTYPE)
+    lib().tos_xibin_finalize(_ptr(out), len(out))
+    return out
+
+
+def brute_run(engine: Engine, points: np.ndarray, rmin: float, rmax: float, nbins: int):
+    """All-pairs isotropic xi(r) (bruteGPU). points: (n, 5) float32 rows x, y, z, delta, w.
+    Returns dsum, wsum, counts (nbins+2 each, bin 0 underflow, nbins+1 overflow) and kernel ms."""
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    if pts.ndim != 2 or pts.shape[1] != 5:
+        raise ValueError("points must be (n, 5)")
+    dsum = np.zeros(nbins + 2)
+    wsum = np.zeros(nbins + 2)
+    counts = np.zeros(nbins + 2, dtype=np.uint64)
+    ms = C.c_double()
+    _check(lib().tos_brute_run(engine.handle, _ptr(pts), len(pts), rmin, rmax, nbins, _ptr(dsum), _ptr(wsum),
+                               _ptr(counts), C.byref(ms)))
+    return dsum, wsum, counts, ms.value
+
+
+def comoving_distance(omega_matter: float, z) -> np.ndarray:
+    z = np.ascontiguousarray(z, dtype=np.float64)
+    out = np.zeros_like(z)
+    _check(lib().tos_comoving_distance(omega_matter, _ptr(z), z.size, _ptr(out)))
+    return out
+
+
+def header_symbols() -> list:
+    """Function names declared in include/tos_b200.h."""
+    import re
+    path = os.path.join(os.path.dirname(PKG_ROOT), "include", "tos_b200.h")
+    text = open(path).read()
+    return sorted(set(re.findall(r"^\s*(?:[a-z_0-9]+\s*\**\s+)+\**\s*(tos_[a-z_0-9]+)\s*\(", text, re.M)))
