@@ -105,6 +105,8 @@ typedef struct {
   uint64_t num_edge_rechecks;        /* pixel pairs re-evaluated in FP64 near a bin edge */
   uint64_t num_index_overflow;       /* pairs whose unchecked z or theta index ran past the grid (dropped) */
   uint64_t num_cells;                /* occupied sky cells */
+  uint64_t num_direct_runs;          /* runs added straight to global memory (outside the shared window) */
+  uint64_t num_window_flushes;       /* shared-window flushes into the per-cell sums */
   double max_ang, cos_max_ang;       /* angular cut actually used (radians) */
   double ms_expand;                  /* device time: sightline-pair expansion */
   double ms_pairs;                   /* device time: pixel-pair kernel */

@@ -64,7 +64,8 @@ def _p(a):
 def xi(sightlines, pixels, order: int, coord: int, axes, scale: float, mode: int = 1, nthreads: int = 0,
        cell_subset=None, subsamples: bool = False, kind: str = "strict"):
     """Oracle pair count.  Returns (bins, cells or None, cell_ids, stats).
-    mode 0: reference arithmetic (float products); mode 1: FP64 sums."""
+    mode 0: reference arithmetic (float products); mode 1: FP64 sums;
+    mode 2: FP64 sums of absolute values of the signed terms."""
     L = lib(kind)
     ra = np.ascontiguousarray(sightlines["ra"], dtype=np.float64)
     dec = np.ascontiguousarray(sightlines["dec"], dtype=np.float64)

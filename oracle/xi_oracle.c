@@ -160,12 +160,12 @@ static void acc_pair(orc_xibin* b, const orc_pixel* i, const orc_pixel* j, int m
     b->wi += i->weight;
     b->wj += j->weight;
     b->z += 0.5 * (i->loglam + j->loglam);
-  } else { /* FP64 */
+  } else { /* FP64; mode 2 sums absolute values (the scale of each signed sum) */
     const double wdi = (double)i->weight * (double)i->value;
     const double wdj = (double)j->weight * (double)j->value;
-    b->didj += wdi * wdj;
-    b->di += wdi;
-    b->dj += wdj;
+    b->didj += (mode == 2) ? fabs(wdi * wdj) : wdi * wdj;
+    b->di += (mode == 2) ? fabs(wdi) : wdi;
+    b->dj += (mode == 2) ? fabs(wdj) : wdj;
     b->wgt += (double)i->weight * (double)j->weight;
     b->wi += (double)i->weight;
     b->wj += (double)j->weight;

@@ -23,11 +23,13 @@ def main():
     for name, g in GRIDS.items():
         bins, cells, ids, st = oracle.xi(los, px, 6, g.type, g.axes_array(), meta["scale"], mode=1,
                                          nthreads=4, subsamples=True)
+        absb = oracle.xi(los, px, 6, g.type, g.axes_array(), meta["scale"], mode=2, nthreads=4)[0]
         out = dict(sightlines=los, pixels=px, order=6, coord=g.type, axes=g.axes_array(),
                    scale=meta["scale"], num_pairs=bins["num_pairs"], cell_ids=ids,
                    cell_num_pairs=cells["num_pairs"])
         for f in FIELDS:
             out[f] = bins[f]
+            out["abs_" + f] = absb[f]
         path = os.path.join(os.path.dirname(__file__), f"golden_{name}.npz")
         np.savez_compressed(path, **out)
         print(path, int(bins["num_pairs"].sum()), "pairs,", len(ids), "cells")

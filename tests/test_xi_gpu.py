@@ -36,6 +36,7 @@ def run_both(engine, los, px, grid, scale, order=6, subsamples=True):
     cat.close()
     obins, ocells, oids, ost = oracle.xi(los, px, order, grid.type, grid.axes_array(), scale, mode=1,
                                          subsamples=subsamples)
+    ost["abs"] = oracle.xi(los, px, order, grid.type, grid.axes_array(), scale, mode=2)[0]
     return bins, cells, ids, st, obins, ocells, oids, ost
 
 
@@ -49,7 +50,7 @@ def test_golden_fixture(engine, name):
     assert_counts_equal(bins, {"num_pairs": z["num_pairs"]})
     assert np.array_equal(cells["num_pairs"], z["cell_num_pairs"])
     ref = {f: z[f] for f in FIELDS}
-    assert_sums_close(bins, ref)
+    assert_sums_close(bins, ref, {f: z["abs_" + f] for f in FIELDS})
     assert st["num_pixel_pairs_used"] == int(z["num_pairs"].sum())
 
 
@@ -61,7 +62,7 @@ def test_parity_vs_oracle(engine, name):
     assert np.array_equal(ids, oids)
     assert_counts_equal(bins, obins)
     assert bins["num_pairs"].sum() > 1000
-    errs = assert_sums_close(bins, obins)
+    errs = assert_sums_close(bins, obins, ost["abs"])
     for c in range(len(ids)):
         assert np.array_equal(cells[c]["num_pairs"], ocells[c]["num_pairs"]), f"cell {ids[c]}"
     assert st["num_sightline_pairs_used"] == ost["num_sightline_pairs_used"]
@@ -78,6 +79,7 @@ def test_fast_path_bit_identical_to_fp64_path(engine, name):
     cat = T.Catalog(engine, los, px, 6)
     fast, fc, _ = T.xi_run(engine, cat, g, meta["scale"], subsamples=True)
     exact, ec, _ = T.xi_run(engine, cat, g, meta["scale"], subsamples=True, exact=True)
+    # same bins -> same runs -> same fixed-point sums: bit-identical
     assert np.array_equal(fast, exact)
     assert np.array_equal(fc, ec)
 
@@ -127,7 +129,7 @@ def test_edge_cases(engine):
     los2[6]["ra"], los2[6]["dec"] = los2[7]["ra"], los2[7]["dec"]  # cos(theta) = 1
     bins, _, _, st, obins, _, _, ost = run_both(engine, los2, px, g, meta["scale"], subsamples=False)
     assert_counts_equal(bins, obins)
-    assert_sums_close(bins, obins)
+    assert_sums_close(bins, obins, ost["abs"])
     px_rev = px.copy()
     for s in range(len(los2)):
         o, n = int(los2[s]["pixel_offset"]), int(los2[s]["num_pixels"])
@@ -135,7 +137,7 @@ def test_edge_cases(engine):
     cat = T.Catalog(engine, los2, px_rev, 6)  # unsorted: no column pruning
     rb, _, rst = T.xi_run(engine, cat, g, meta["scale"])
     assert_counts_equal(rb, obins)
-    assert_sums_close(rb, obins)
+    assert_sums_close(rb, obins, ost["abs"])
     assert rst["num_pixel_pairs_evaluated"] == rst["num_pixel_pairs"]
 
 
@@ -158,9 +160,9 @@ def test_pixels_on_bin_edges(engine):
         px[s * npx:(s + 1) * npx]["weight"] = rng.uniform(0.5, 2, npx).astype(np.float32)
     for name in ("cartesian", "polar", "cartesian_offset"):
         g = ALL_GRIDS[name]
-        bins, _, _, st, obins, _, _, _ = run_both(engine, los, px, g, 3586.0, subsamples=False)
+        bins, _, _, st, obins, _, _, ost = run_both(engine, los, px, g, 3586.0, subsamples=False)
         assert_counts_equal(bins, obins)
-        assert_sums_close(bins, obins)
+        assert_sums_close(bins, obins, ost["abs"])
 
 
 def test_invalid_inputs(engine):
@@ -194,7 +196,9 @@ def test_full_size_small_config_cell_subset(engine):
     subset = np.sort(rng.choice(len(ids), size=4, replace=False))
     _, ocells, oids, _ = oracle.xi(los, px, 6, g.type, g.axes_array(), meta["scale"], mode=1,
                                    cell_subset=subset, subsamples=True)
+    _, acells, _, _ = oracle.xi(los, px, 6, g.type, g.axes_array(), meta["scale"], mode=2,
+                                cell_subset=subset, subsamples=True)
     assert np.array_equal(ids, oids)
     for c in subset:
         assert_counts_equal(cells[c], ocells[c])
-        assert_sums_close(cells[c], ocells[c])
+        assert_sums_close(cells[c], ocells[c], acells[c])

@@ -80,6 +80,9 @@ __global__ void k_prep(const tos_pixel* raw, const uint64_t* off, const uint32_t
         mw = fmax(mw, fabs(v1));
         ml = fmax(ml, fabs(v2));
         md = fmax(md, fabs((double)px.distance));
+        if (!isfinite(px.value) || !isfinite(px.weight) || !isfinite(px.loglam) ||
+            !isfinite(px.distance))
+          atomicOr(flags, 2u);
         if (k + 1 < n) {
           const tos_pixel nx = raw[o + k + 1];
           if (!(nx.distance >= px.distance) || !(nx.loglam >= px.loglam)) unsorted = true;
@@ -231,23 +234,25 @@ __global__ void k_expand(const uint32_t* members, uint32_t n_members, const uint
 
 // ---- results ----------------------------------------------------------------
 
-// Per bin: convert every cell's fixed-point sums to double and add them in
-// ascending cell order (the order of xi_finalize_task, XiEstimator.cc:298-305).
-__global__ void k_combine(const long long* acc, uint32_t n_cells, uint32_t nb, double4 inv_a,
-                          double4 inv_b, tos_xibin* out, tos_xibin* cells_out) {
+// Per bin: convert every cell's 128-bit fixed-point sums to double and add
+// them in ascending cell order (the order of xi_finalize_task,
+// XiEstimator.cc:298-305).
+__global__ void k_combine(const unsigned long long* acc, uint32_t n_cells, uint32_t nb,
+                          double4 inv_a, double4 inv_b, tos_xibin* out, tos_xibin* cells_out) {
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
     const double inv[7] = {inv_a.x, inv_a.y, inv_a.z, inv_a.w, inv_b.x, inv_b.y, inv_b.z};
     double s[7] = {0, 0, 0, 0, 0, 0, 0};
     long long n = 0;
     for (uint32_t c = 0; c < n_cells; ++c) {
-      const long long* a = acc + ((size_t)c * nb + b) * 8;
+      const unsigned long long* a = acc + ((size_t)c * nb + b) * kAccWords;
       double v[7];
 #pragma unroll
       for (int k = 0; k < 7; ++k) {
-        v[k] = (double)a[k] * inv[k];
+        // value = hi * 2^64 + lo (lo unsigned)
+        v[k] = __fma_rn((double)(long long)a[7 + k], 18446744073709551616.0, (double)a[k]) * inv[k];
         s[k] += v[k];
       }
-      n += a[7];
+      n += (long long)a[14];
       if (cells_out) {
         tos_xibin x;
         x.didj = v[0];
@@ -257,7 +262,7 @@ __global__ void k_combine(const long long* acc, uint32_t n_cells, uint32_t nb, d
         x.wi = v[4];
         x.wj = v[5];
         x.z = v[6];
-        x.num_pairs = a[7];
+        x.num_pairs = (long long)a[14];
         cells_out[(size_t)c * nb + b] = x;
       }
     }
@@ -430,6 +435,7 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
   DeviceGuard g(e->device);
   std::unique_ptr<tos_catalog> cat(new tos_catalog());
   cat->eng = e;
+  cat->device = e->device;
   cat->n_los = n_los;
   cat->order = order;
   cat->nside = (int64_t)1 << order;
@@ -567,7 +573,7 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
   cat->max_w = maxes[1];
   cat->max_l = maxes[2];
   cat->max_d = maxes[3];
-  if (!std::isfinite(cat->max_abs_wd) || !std::isfinite(cat->max_w) ||
+  if ((flags & 2u) || !std::isfinite(cat->max_abs_wd) || !std::isfinite(cat->max_w) ||
       !std::isfinite(cat->max_l) || !std::isfinite(cat->max_d))
     return fail(TOS_ERR_INVALID_ARG,
                 "pixels must have finite value, weight, loglam and distance (filter them as "
@@ -580,9 +586,8 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
 
 void tos_catalog_destroy(tos_catalog* c) {
   if (!c) return;
-  DeviceGuard g(c->eng->device);
-  cudaStreamSynchronize(c->eng->stream);
-  delete c;
+  DeviceGuard g(c->device);
+  delete c;  // cudaFree synchronises with pending work on the device
 }
 
 tos_status tos_catalog_num_cells(const tos_catalog* c, size_t* n) {
@@ -750,7 +755,7 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   TOS_CUDA_TRY(cudaEventRecord(e->ev[1], st));
 
   // --- accumulation layout and fixed-point scales
-  const size_t acc_words = (size_t)nc * nb * 8;
+  const size_t acc_words = (size_t)nc * nb * kAccWords;
   TOS_TRY(cat->d_acc.alloc(acc_words));
   TOS_CUDA_TRY(cudaMemsetAsync(cat->d_acc.p, 0, acc_words * 8, st));
   PairArgs A{};
@@ -773,21 +778,22 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   A.acc = cat->d_acc.p;
   A.counters = ctr;
   A.force_exact = (flags & TOS_XI_EXACT) ? 1 : 0;
-  // fixed point: 2^F per field, F = min(window bound, per-cell bound)
+  // fixed point: 2^F per field.  A run contributes c with |c| <= bound
+  // (a run has at most max_np pixels).  Signed sums (didj, di, dj) use
+  // |round(c 2^F)| < 2^62 split into 22+22+18-bit words, positive sums
+  // |round(c 2^F)| < 2^42 split into 22+20-bit words; a window slot takes at
+  // most 1024 contributions, and the per-cell accumulators are 128-bit.
   {
     const double m = std::max<double>(1.0, cat->max_np);
     const double wdm = std::max(cat->max_abs_wd, 1e-300), wm = std::max(cat->max_w, 1e-300),
                  lm = std::max(cat->max_l, 1e-300);
-    const double per_contrib[7] = {wdm * m * wdm, wdm * m, m * wdm, wm * m * wm, wm * m, m * wm,
-                                   lm * m};
-    const double per_pair[7] = {wdm * wdm, wdm, wdm, wm * wm, wm, wm, lm};
-    const double cp = std::max<double>(1.0, (double)max_cell_pairs);
+    const double bound[7] = {wdm * m * wdm, wdm * m, m * wdm, wm * m * wm, wm * m, m * wm, lm * m};
     for (int k = 0; k < 7; ++k) {
-      const double f1 = 38.0 - std::log2(per_contrib[k]);
-      const double f2 = 62.0 - std::log2(cp * per_pair[k]);
-      int f = (int)std::floor(std::min(f1, f2));
+      const double top = (k < kSigned) ? 62.0 : 42.0;
+      int f = (int)std::floor(top - std::log2(bound[k]));
       f = std::max(-60, std::min(f, 200));
       A.scale[k] = std::ldexp(1.0, f);
+      if (k < kSigned) A.scale_hi[k] = std::ldexp(1.0, f - 44);
     }
   }
   // FP32 fast-path constants
@@ -833,27 +839,20 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
     A.win_lim = lim;
     if (!std::isfinite(lim)) A.prune = 0;
   }
-  // window layout
-  if (G.type == TOS_CARTESIAN) {
-    A.win_w1 = (int)std::min<uint32_t>(8u, rg.n1);
-    A.win_slots = (int)(n0 * (uint32_t)A.win_w1);
-  } else if (G.type == TOS_POLAR) {
-    A.win_w1 = 0;
-    A.win_slots = (int)std::min<uint32_t>(n0 * rg.n1, 400u);
-  } else {
-    A.win_w1 = 0;
-    A.win_slots = (int)n0;
-  }
-  if ((size_t)A.win_slots * kWinWords * 4 * kPairWarps > 200 * 1024) {
-    // very long first axis: keep only part of it in the window, the rest goes direct
-    A.win_slots = (int)(200 * 1024 / (kWinWords * 4 * kPairWarps));
-    if (G.type == TOS_CARTESIAN) A.win_w1 = std::max(1, A.win_slots / (int)n0);
-    if (G.type == TOS_CARTESIAN && (uint32_t)A.win_w1 * n0 > (uint32_t)A.win_slots) A.win_w1 = 0;
-  }
-  A.contrib_limit = 120;
-  if (cat->max_np > 0) {
-    const uint64_t lim_count = 0xFFFFFFFFull / ((uint64_t)32 * (cat->max_np + 1)) ;
-    if (lim_count < A.contrib_limit) A.contrib_limit = (uint32_t)std::max<uint64_t>(1, lim_count - 1);
+  // window layout: per warp, slots of kWinWords u32 words within ~200 KB per CTA
+  {
+    const int budget = (int)(200 * 1024 / ((size_t)kWinWords * 4 * kPairWarps));
+    if (G.type == TOS_CARTESIAN) {
+      A.win_w1 = (int)std::min<uint32_t>(4u, rg.n1);
+      if ((int)n0 * A.win_w1 > budget) A.win_w1 = std::max(0, budget / (int)n0);
+      A.win_slots = std::max(1, (int)n0 * A.win_w1);
+    } else if (G.type == TOS_POLAR) {
+      A.win_w1 = 0;
+      A.win_slots = (int)std::min<uint32_t>(n0 * rg.n1, (uint32_t)budget);
+    } else {
+      A.win_w1 = 0;
+      A.win_slots = (int)std::min<uint32_t>(n0, (uint32_t)budget);
+    }
   }
   if (n_items > 0) {
     TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
@@ -879,8 +878,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   if (want_cells)
     TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, cat->d_out.p + nb, (size_t)nc * nb * sizeof(tos_xibin),
                                  cudaMemcpyDeviceToHost, st));
-  unsigned long long hc[4];
-  TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, 32, cudaMemcpyDeviceToHost, st));
+  unsigned long long hc[8];
+  TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, 64, cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
   if (stats) {
@@ -896,6 +895,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
     stats->num_pixel_pairs_evaluated = hc[0];
     stats->num_edge_rechecks = hc[1];
     stats->num_index_overflow = hc[2];
+    stats->num_direct_runs = hc[3];
+    stats->num_window_flushes = hc[6];
     stats->num_cells = nc;
     stats->max_ang = max_ang;
     stats->cos_max_ang = cos_max;

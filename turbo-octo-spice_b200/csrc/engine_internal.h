@@ -71,6 +71,7 @@ struct tos_engine {
 
 struct tos_catalog {
   tos_engine* eng = nullptr;
+  int device = 0;
   size_t n_los = 0, n_pix = 0;
   int order = 0;
   int64_t nside = 0;
@@ -106,7 +107,7 @@ struct tos_catalog {
   tos::DevBuf<uint32_t> d_item_i, d_item_j, d_item_sep;
   tos::DevBuf<double> d_item_c;
   tos::DevBuf<unsigned long long> d_cell_pairs;        // per cell sum N_i N_j
-  tos::DevBuf<long long> d_acc;                        // [n_cells][n_bins][8] fixed point
+  tos::DevBuf<unsigned long long> d_acc;               // [n_cells][n_bins][16] 128-bit fixed point
   tos::DevBuf<tos_xibin> d_out;                        // combined / per cell output
   tos::DevBuf<unsigned long long> d_counters;          // misc counters
   tos::DevBuf<unsigned char> d_cub_tmp;

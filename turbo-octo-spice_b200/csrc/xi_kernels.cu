@@ -24,6 +24,31 @@ __device__ __forceinline__ long long to_fixed(double c, double scale) {
   return __double_as_longlong(__fma_rn(c, scale, kMagic52)) - kMagic52Bits;
 }
 
+// round(c * 2^F) for |c * 2^F| < 2^62, given sh = 2^(F-44): the high part is
+// rounded first and the exact remainder carries the low 44 bits.
+__device__ __forceinline__ long long to_fixed_wide(double c, double sh) {
+  const double v = c * sh;
+  const long long qh = __double_as_longlong(__dadd_rn(v, kMagic52)) - kMagic52Bits;
+  const double rem = v - (double)qh;  // exact, |rem| <= 0.5
+  return (qh << 44) + to_fixed(rem, 17592186044416.0 /* 2^44 */);
+}
+
+// Window word of field k, part p (0 = low).
+__device__ __forceinline__ int wword(int k, int p) {
+  return (k < kSigned) ? 3 * k + p : 3 * kSigned + 2 * (k - kSigned) + p;
+}
+constexpr int kWordCount = 3 * kSigned + 2 * (7 - kSigned);      // 17
+constexpr int kWordContrib = kWordCount + 1;                     // 18
+
+// Add a signed 64-bit value to a 128-bit accumulator {lo: u64, hi: i64}.
+__device__ __forceinline__ void add128(unsigned long long* lo, unsigned long long* hi, long long q) {
+  const unsigned long long uq = (unsigned long long)q;
+  const unsigned long long old = atomicAdd(lo, uq);
+  const long long carry = (old + uq < old) ? 1 : 0;
+  const long long h = (q < 0 ? -1 : 0) + carry;
+  if (h != 0) atomicAdd(hi, (unsigned long long)h);
+}
+
 // ---- exact re-binning (reference expression order) returning the two axis
 // indices; z is handled per item.  Mirrors ref_bin_* in tos_common.h.
 __device__ __forceinline__ bool exact_cart(float d1, float d2, double c, const RefGrid& g,
@@ -87,7 +112,7 @@ struct Item {
   uint32_t zb;       // constant z index of the item
   uint32_t sep;      // observing: theta index
   int zconst;        // z index constant over the item
-  int lo1;           // Cartesian window: first axis-1 bin
+  int lo1;           // Cartesian window: first axis-1 bin of the current chunk
   const float* colx; // padded column coordinate (distance or loglam) of sightline j
   const float* coll; // padded column loglam
   const float* cold; // padded column distance
@@ -117,18 +142,25 @@ __device__ __forceinline__ uint32_t flat_index(const PairArgs& A, const Item& it
   return it.zb + b * A.g.n2;
 }
 
-// Add one run's contribution directly to the global per-cell accumulator.
-__device__ __forceinline__ void add_direct(const PairArgs& A, uint32_t cell, uint32_t idx,
-                                           const double* c, uint32_t m) {
+__device__ __forceinline__ unsigned long long* acc_base(const PairArgs& A, uint32_t cell,
+                                                        uint32_t idx) {
+  return A.acc + ((size_t)cell * A.g.ntotal + idx) * kAccWords;
+}
+
+// Add one run's contribution directly to the global per-cell accumulator
+// (keys outside the window, and the all-FP64 validation path).
+__device__ void add_direct(const PairArgs& A, uint32_t cell, uint32_t idx, const double* c,
+                           uint32_t m) {
   if (idx >= A.g.ntotal) {
     atomicAdd(&A.counters[2], (unsigned long long)m);
     return;
   }
-  unsigned long long* base =
-      (unsigned long long*)(A.acc + ((size_t)cell * A.g.ntotal + idx) * 8);
+  unsigned long long* base = acc_base(A, cell, idx);
 #pragma unroll
-  for (int k = 0; k < 7; ++k) atomicAdd(base + k, (unsigned long long)to_fixed(c[k], A.scale[k]));
-  atomicAdd(base + 7, (unsigned long long)m);
+  for (int k = 0; k < 7; ++k)
+    add128(base + k, base + 7 + k,
+           k < kSigned ? to_fixed_wide(c[k], A.scale_hi[k]) : to_fixed(c[k], A.scale[k]));
+  atomicAdd(base + 14, (unsigned long long)m);
   atomicAdd(&A.counters[3], 1ull);
 }
 
@@ -141,8 +173,9 @@ __device__ void flush_window(const PairArgs& A, const Item& it, uint32_t* win, i
                                    : (int)A.g.n0;
   if (nslots > S) nslots = S;
   for (int s = lane; s < nslots; s += 32) {
-    const uint32_t cnt = win[14 * S + s];
-    if (cnt == 0) continue;
+    const uint32_t contrib = win[kWordContrib * S + s];
+    if (contrib == 0) continue;
+    const uint32_t cnt = win[kWordCount * S + s];
     uint32_t key;
     if (COORD == kCart)
       key = ((uint32_t)(s / A.win_w1) << 16) | (uint32_t)(it.lo1 + s % A.win_w1);
@@ -152,22 +185,33 @@ __device__ void flush_window(const PairArgs& A, const Item& it, uint32_t* win, i
       key = (uint32_t)s << 16;
     const uint32_t idx = flat_index<COORD>(A, it, key);
     if (idx < A.g.ntotal) {
-      unsigned long long* base =
-          (unsigned long long*)(A.acc + ((size_t)it.cell * A.g.ntotal + idx) * 8);
+      unsigned long long* base = acc_base(A, it.cell, idx);
 #pragma unroll
       for (int k = 0; k < 7; ++k) {
-        const uint32_t lo = win[(2 * k) * S + s];
-        const int hi = (int)win[(2 * k + 1) * S + s];
-        const long long q = ((long long)hi << kSplit) + (long long)lo;
-        atomicAdd(base + k, (unsigned long long)q);
+        const uint32_t lo = win[wword(k, 0) * S + s];
+        if (k < kSigned) {
+          // value = hi * 2^44 + mid * 2^22 + lo as a 128-bit number
+          const uint32_t mid = win[wword(k, 1) * S + s];
+          const int hi = (int)win[wword(k, 2) * S + s];
+          const unsigned long long l0 = (unsigned long long)lo + ((unsigned long long)mid << kSplit);
+          const unsigned long long l1 = l0 + ((unsigned long long)(hi & 0xFFFFF) << 44);
+          const long long h = (long long)(hi >> 20) + (l1 < l0 ? 1 : 0);
+          const unsigned long long old = atomicAdd(base + k, l1);
+          const long long hh = h + ((old + l1 < old) ? 1 : 0);
+          if (hh != 0) atomicAdd(base + 7 + k, (unsigned long long)hh);
+        } else {
+          const int hi = (int)win[wword(k, 1) * S + s];
+          add128(base + k, base + 7 + k, ((long long)hi << kSplit) + (long long)lo);
+        }
       }
-      atomicAdd(base + 7, (unsigned long long)cnt);
+      atomicAdd(base + 14, (unsigned long long)cnt);
     } else {
       atomicAdd(&A.counters[2], (unsigned long long)cnt);
     }
 #pragma unroll
     for (int w = 0; w < kWinWords; ++w) win[w * S + s] = 0u;
   }
+  if (lane == 0) atomicAdd(&A.counters[6], 1ull);
   __syncwarp();
 }
 
@@ -219,13 +263,13 @@ __device__ __forceinline__ void fast_bin(const PairArgs& A, const Row& R, float 
 // Exact (FP64 reference) key of one pair.
 template <int COORD>
 __device__ __forceinline__ uint32_t exact_key(const PairArgs& A, const Row& R, const Item& it,
-                                              float x2, float d2) {
+                                              float x2) {
   uint32_t b0 = 0, b1 = 0;
   bool ok;
   if (COORD == kCart)
-    ok = exact_cart(R.d1, d2, it.c, A.g, &b0, &b1);
+    ok = exact_cart(R.d1, x2, it.c, A.g, &b0, &b1);
   else if (COORD == kPolar)
-    ok = exact_polar(R.d1, d2, it.c, A.g, &b0, &b1);
+    ok = exact_polar(R.d1, x2, it.c, A.g, &b0, &b1);
   else
     ok = exact_obs(R.x1, x2, A.g, &b0);
   return ok ? ((b0 << 16) | b1) : kInvalidKey;
@@ -234,7 +278,7 @@ __device__ __forceinline__ uint32_t exact_key(const PairArgs& A, const Row& R, c
 // Exact flat key including a per-pair z index (items whose z index varies).
 template <int COORD>
 __device__ __forceinline__ uint32_t exact_flat_key(const PairArgs& A, const Row& R, const Item& it,
-                                                   float x2, float d2, float l2) {
+                                                   float d2, float l2) {
   uint32_t idx = 0;
   bool ok;
   if (COORD == kCart)
@@ -247,91 +291,150 @@ __device__ __forceinline__ uint32_t exact_flat_key(const PairArgs& A, const Row&
   return ok ? (idx == kInvalidKey ? kInvalidKey - 1u : idx) : kInvalidKey;
 }
 
+// Contribution of one closed run to the seven XiBin sums and the count.
+struct Contrib {
+  double c[7];
+  uint32_t m;
+};
+
+__device__ __forceinline__ void make_contrib(const Row& R, uint32_t m, double dwd, double dw,
+                                             double dl, Contrib& o) {
+  const double md = (double)m;
+  o.m = m;
+  o.c[0] = R.wd1 * dwd;
+  o.c[1] = R.wd1 * md;
+  o.c[2] = dwd;
+  o.c[3] = R.w1 * dw;
+  o.c[4] = R.w1 * md;
+  o.c[5] = dw;
+  o.c[6] = __fma_rn(R.hl1, md, 0.5 * dl);
+}
+
+// Add the runs closed by lanes with `emit` into the warp window: lanes that
+// close a run in the same slot are summed with redux.sync and one of them adds
+// the sums.  Keys outside the window go straight to the global accumulators.
+// Returns (warp-uniform) whether some slot reached its capacity.
+template <int COORD>
+__device__ __forceinline__ bool emit_runs(const PairArgs& A, const Item& it, uint32_t* win,
+                                          int lane, bool emit, uint32_t key, const Contrib& ct) {
+  int slot = -1;
+  if (emit) {
+    slot = window_slot<COORD>(A, it, key);
+    if (slot < 0) add_direct(A, it.cell, flat_index<COORD>(A, it, key), ct.c, ct.m);
+  }
+  unsigned pending = __ballot_sync(kFull, emit && slot >= 0);
+  bool full = false;
+  if (pending) {
+    uint32_t wv[kWordCount];
+    if (emit && slot >= 0) {
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+        if (k < kSigned) {
+          const long long q = to_fixed_wide(ct.c[k], A.scale_hi[k]);
+          wv[wword(k, 0)] = (uint32_t)q & ((1u << kSplit) - 1u);
+          wv[wword(k, 1)] = (uint32_t)(q >> kSplit) & ((1u << kSplit) - 1u);
+          wv[wword(k, 2)] = (uint32_t)(int)(q >> (2 * kSplit));
+        } else {
+          const long long q = to_fixed(ct.c[k], A.scale[k]);
+          wv[wword(k, 0)] = (uint32_t)q & ((1u << kSplit) - 1u);
+          wv[wword(k, 1)] = (uint32_t)(int)(q >> kSplit);
+        }
+      }
+    }
+    const int S = A.win_slots;
+    while (pending) {
+      const int leader = __ffs(pending) - 1;
+      const int ls = __shfl_sync(kFull, slot, leader);
+      const unsigned peers = __ballot_sync(kFull, ((pending >> lane) & 1u) && slot == ls);
+      if ((peers >> lane) & 1u) {
+        const bool lead = lane == leader;
+#pragma unroll
+        for (int w = 0; w < kWordCount; ++w) {
+          const uint32_t sw = __reduce_add_sync(peers, wv[w]);
+          if (lead) atomicAdd(&win[w * S + ls], sw);
+        }
+        const uint32_t sm = __reduce_add_sync(peers, ct.m);
+        if (lead) {
+          atomicAdd(&win[kWordCount * S + ls], sm);
+          const uint32_t n = (uint32_t)__popc(peers);
+          const uint32_t old = atomicAdd(&win[kWordContrib * S + ls], n);
+          full = old + n > kSlotCap;
+        }
+      }
+      pending &= ~peers;
+    }
+  }
+  return __any_sync(kFull, full);
+}
+
 // Sweep one 32-row chunk.  MODE 0: fast path with packed keys and the warp
 // window; MODE 1: every pair exact, flat keys, direct global adds.
 template <int COORD, bool EXACT0, bool MINPOS, int MODE>
 __device__ void sweep_chunk(const PairArgs& A, const Item& it, const Row& R, bool active,
                             int t_begin, int t_end, uint32_t* win, int lane,
-                            unsigned long long& n_recheck, uint32_t& ncontrib) {
+                            unsigned long long& n_recheck) {
   uint32_t cur = kInvalidKey;
   int run_start = 0;
   double ps0 = 0, ps1 = 0, ps2 = 0;
-
-  auto close_run = [&](int p_end, const double4& pn) {
-    const uint32_t m = (uint32_t)(p_end - run_start);
-    const double md = (double)m;
-    const double dwd = pn.x - ps0, dw = pn.y - ps1, dl = pn.z - ps2;
-    double c[7];
-    c[0] = R.wd1 * dwd;
-    c[1] = R.wd1 * md;
-    c[2] = dwd;
-    c[3] = R.w1 * dw;
-    c[4] = R.w1 * md;
-    c[5] = dw;
-    c[6] = __fma_rn(R.hl1, md, 0.5 * dl);
-    if (MODE == 0) {
-      const int slot = window_slot<COORD>(A, it, cur);
-      if (slot >= 0) {
-        const int S = A.win_slots;
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-          const long long q = to_fixed(c[k], A.scale[k]);
-          atomicAdd(&win[(2 * k) * S + slot], (uint32_t)q & ((1u << kSplit) - 1u));
-          atomicAdd(&win[(2 * k + 1) * S + slot], (uint32_t)(int)(q >> kSplit));
-        }
-        atomicAdd(&win[14 * S + slot], m);
-        ++ncontrib;
-      } else {
-        add_direct(A, it.cell, flat_index<COORD>(A, it, cur), c, m);
-      }
-    } else {
-      add_direct(A, it.cell, cur, c, m);
-    }
-  };
-
+  float x2n = it.colx[t_begin + lane];
   for (int t = t_begin; t < t_end; ++t) {
     const int p2 = t + lane;
-    const float x2 = it.colx[p2];
+    const float x2 = x2n;
+    x2n = it.colx[p2 + 1];  // next step (p2 + 1 <= nj + 31: inside the padding)
     uint32_t key;
-    bool recheck;
     if (MODE == 0) {
+      bool recheck;
       fast_bin<COORD, EXACT0, MINPOS>(A, R, x2, key, recheck);
       if (__any_sync(kFull, recheck)) {
         if (recheck) {
-          key = exact_key<COORD>(A, R, it, x2, (COORD == kObs) ? 0.f : x2);
+          key = exact_key<COORD>(A, R, it, x2);
           ++n_recheck;
         }
       }
     } else {
       key = kInvalidKey;
-      if (active && p2 >= 0 && p2 < (int)it.nj) {
-        const float d2 = it.cold[p2], l2 = it.coll[p2];
-        key = exact_flat_key<COORD>(A, R, it, x2, d2, l2);
-      }
+      if (active && p2 >= 0 && p2 < (int)it.nj)
+        key = exact_flat_key<COORD>(A, R, it, it.cold[p2], it.coll[p2]);
     }
     const bool changed = key != cur;
     if (__any_sync(kFull, changed)) {
+      Contrib ct;
+      bool emit = false;
       if (changed) {
         const int pc = min(max(p2, 0), (int)it.nj);
         const double4 pn = it.pre[pc];
-        if (cur != kInvalidKey) close_run(p2, pn);
-        cur = key;
-        run_start = p2;
+        if (cur != kInvalidKey) {
+          emit = true;
+          make_contrib(R, (uint32_t)(p2 - run_start), pn.x - ps0, pn.y - ps1, pn.z - ps2, ct);
+        }
         ps0 = pn.x;
         ps1 = pn.y;
         ps2 = pn.z;
       }
-      if (MODE == 0 && __any_sync(kFull, ncontrib >= A.contrib_limit)) {
-        flush_window<COORD>(A, it, win, lane);
-        ncontrib = 0;
+      if (MODE == 0) {
+        if (emit_runs<COORD>(A, it, win, lane, emit, cur, ct)) flush_window<COORD>(A, it, win, lane);
+      } else if (emit) {
+        add_direct(A, it.cell, cur, ct.c, ct.m);
+      }
+      if (changed) {
+        cur = key;
+        run_start = p2;
       }
     }
   }
   // close runs still open at the end of the sweep
-  if (cur != kInvalidKey) {
+  Contrib ct;
+  const bool emit = cur != kInvalidKey;
+  if (emit) {
     const int p_end = t_end + lane;
-    const int pc = min(max(p_end, 0), (int)it.nj);
-    close_run(p_end, it.pre[pc]);
+    const double4 pn = it.pre[min(max(p_end, 0), (int)it.nj)];
+    make_contrib(R, (uint32_t)(p_end - run_start), pn.x - ps0, pn.y - ps1, pn.z - ps2, ct);
+  }
+  if (MODE == 0) {
+    emit_runs<COORD>(A, it, win, lane, emit, cur, ct);
+    flush_window<COORD>(A, it, win, lane);
+  } else if (emit) {
+    add_direct(A, it.cell, cur, ct.c, ct.m);
   }
 }
 
@@ -358,7 +461,7 @@ __device__ void process_item(const PairArgs& A, Item& it, uint32_t* win, int lan
   const float* rowl = A.loglam_pad + oi + (uint64_t)kPad * (it.i + 1);
   const double* rowwd = A.wd + oi;
   const float* roww = A.w + oi;
-  uint32_t ncontrib = 0;  // window contributions of this lane since the last flush
+  const float4 rj = A.range[it.j];
   for (uint32_t r0 = 0; r0 < it.ni; r0 += 32) {
     const uint32_t row = r0 + lane;
     const bool active = row < it.ni;
@@ -417,10 +520,18 @@ __device__ void process_item(const PairArgs& A, Item& it, uint32_t* win, int lan
       const int a = max(t_begin + (int)lane, 0), b = min(t_end + (int)lane, (int)it.nj);
       if (b > a) n_eval += (unsigned long long)(b - a);
     }
-    sweep_chunk<COORD, EXACT0, MINPOS, MODE>(A, it, R, active, t_begin, t_end, win, lane,
-                                            n_recheck, ncontrib);
+    if (COORD == kCart && MODE == 0) {
+      // window along axis 1: lowest r_perp bin of the chunk, from its smallest
+      // row distance (lane 0 when sorted) and the smallest column distance,
+      // less the float rounding of d1*d1; keys below it go direct
+      const float d1min = __shfl_sync(kFull, R.d1, 0);
+      const float u = it.ap * d1min * rj.x * (1.f - 1e-5f) -
+                      ldexpf(d1min * d1min * A.inv1sqf, -22);
+      const int lo1 = (int)floorf(sqrtf(fmaxf(u, 0.f)) + A.off1f - 1e-2f);
+      it.lo1 = max(0, min(lo1, (int)A.g.n1 - 1));
+    }
+    sweep_chunk<COORD, EXACT0, MINPOS, MODE>(A, it, R, active, t_begin, t_end, win, lane, n_recheck);
   }
-  if (MODE == 0) flush_window<COORD>(A, it, win, lane);
 }
 
 template <int COORD, bool EXACT0, bool MINPOS>
@@ -459,16 +570,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) pair_kernel(PairArgs A) {
     const double zhi = dmul(dsub(dmul(0.5, (double)lsum_hi), A.g.min2), A.g.invn2);
     it.zb = zbin_of_sum(lsum_lo, A.g);
     it.zconst = (zlo > -1.0 && zhi < 2147483648.0 && it.zb == zbin_of_sum(lsum_hi, A.g)) ? 1 : 0;
-    // Cartesian window along axis 1 from the distance ranges
     it.lo1 = 0;
-    if (COORD == kCart) {
-      const float ulo = it.ap * ri.x * rj.x, uhi = it.ap * ri.y * rj.y;
-      const float slack = 1e-3f + 2e-7f * (ri.y * ri.y) * A.inv1sqf;
-      const float tlo = sqrtf(fmaxf(ulo * (1.f - 1e-5f) - slack, 0.f)) + A.off1f;
-      int lo1 = (int)floorf(tlo - 1e-2f);
-      it.lo1 = max(0, min(lo1, (int)A.g.n1 - 1));
-      (void)uhi;
-    }
     const bool exact_item = A.force_exact || !it.zconst;
     if (exact_item)
       process_item<COORD, EXACT0, MINPOS, 1>(A, it, win, lane, n_eval, n_recheck);

@@ -14,13 +14,14 @@
 //      reference's exact FP64 expression order;
 //   4. each lane keeps a run of consecutive columns with the same bin; when the
 //      bin changes, the run's contribution to all eight XiBin fields comes
-//      from FP64 prefix sums of sightline j, is quantised to 64-bit fixed point
-//      and added with two u32 shared-memory atomics per field into the warp's
-//      private window (u32 adds are native; aligned lanes hit the same slot
-//      and are combined by the hardware);
-//   5. at the end of the item the window is added into per-cell int64
-//      accumulators in global memory, so every sum is exact, deterministic
-//      and independent of scheduling.
+//      from FP64 prefix sums of sightline j and is quantised to fixed point
+//      (two u32 words per field); the lanes that close a run in the same slot
+//      are summed with warp reductions (redux.sync) and one lane adds the sums
+//      into the warp's private window in shared memory (u32 adds are native,
+//      and aligned lanes would otherwise serialise on one address);
+//   5. at the end of every 32-row chunk the window is added into per-cell
+//      128-bit fixed-point accumulators in global memory, so every sum is
+//      exact, deterministic and independent of scheduling.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -32,9 +33,16 @@
 namespace tos {
 
 constexpr uint32_t kInvalidKey = 0xFFFFFFFFu;
-constexpr int kPairWarps = 8;   // warps per CTA of the pair kernel
-constexpr int kWinWords = 15;   // u32 words per window slot: 7 x (lo, hi) + count
-constexpr int kSplit = 20;      // bits in the low word of the fixed-point split
+constexpr int kPairWarps = 12;  // warps per CTA of the pair kernel
+// u32 words per window slot: the three signed sums (didj, di, dj) as 22+22+rest
+// bit words of a 62-bit fixed-point value, the four positive sums (wgt, wi,
+// wj, z) as 22+rest bit words of a 42-bit value, the pair count and the
+// number of contributions.
+constexpr int kWinWords = 19;
+constexpr int kSplit = 22;      // bits in each low word of the fixed-point split
+constexpr int kSigned = 3;      // fields 0..2 are signed (3 words), 3..6 positive (2 words)
+constexpr uint32_t kSlotCap = 1024u - 64u;  // contributions per slot before the window is emptied
+constexpr int kAccWords = 16;   // u64 words per (cell, bin): 7 lo, 7 hi, count, unused
 constexpr double kMagic52 = 6755399441055744.0;  // 1.5 * 2^52
 constexpr long long kMagic52Bits = 0x4338000000000000LL;
 
@@ -69,11 +77,12 @@ struct PairArgs {
   int prune;                 // sightlines sorted: restrict columns to the r_par window
   // accumulation
   double scale[7];           // 2^F per field
+  double scale_hi[3];        // 2^(F-44) for the signed fields
   int win_w1;                // window width along axis 1 (Cartesian)
   int win_slots;             // slots per warp window
-  uint32_t contrib_limit;    // contributions per lane before a window flush
-  long long* acc;            // [n_cells][ntotal][8] fixed point
-  unsigned long long* counters;  // [0] evaluated pairs [1] rechecks [2] overflow pairs [3] direct runs
+  unsigned long long* acc;   // [n_cells][ntotal][kAccWords] 128-bit fixed point
+  unsigned long long* counters;  // [0] evaluated pairs [1] rechecks [2] overflow pairs
+                                 // [3] direct runs [4] item counter [6] window flushes
   int force_exact;           // evaluate every pixel pair with the FP64 reference
 };
 

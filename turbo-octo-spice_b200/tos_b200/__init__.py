@@ -50,7 +50,7 @@ class XiStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "num_sightlines", "num_sightline_pairs", "num_sightline_pairs_used", "num_pixels",
         "num_pixel_pairs", "num_pixel_pairs_used", "num_pixel_pairs_evaluated", "num_edge_rechecks",
-        "num_index_overflow", "num_cells")] + [(n, C.c_double) for n in (
+        "num_index_overflow", "num_cells", "num_direct_runs", "num_window_flushes")] + [(n, C.c_double) for n in (
             "max_ang", "cos_max_ang", "ms_expand", "ms_pairs", "ms_total", "ms_device")]
 
     def as_dict(self) -> dict:
@@ -182,7 +182,10 @@ class Engine:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def __enter__(self):
         return self
@@ -230,7 +233,10 @@ class Catalog:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def xi_run(engine: Engine, catalog: Catalog, grid: Grid, scale: float, subsamples: bool = False,
