@@ -109,9 +109,11 @@ typedef struct {
   uint64_t num_window_flushes;       /* shared-window flushes into the per-cell sums */
   double max_ang, cos_max_ang;       /* angular cut actually used (radians) */
   double ms_expand;                  /* device time: sightline-pair expansion */
-  double ms_pairs;                   /* device time: pixel-pair kernel */
+  double ms_pairs;                   /* device time: run-sweep and pixel-pair kernels */
   double ms_total;                   /* wall time of the call */
   double ms_device;                  /* device time of the whole call (expansion to results) */
+  uint64_t num_run_items;            /* sightline pairs counted by the run-sweep kernel */
+  double ms_runs;                    /* device time: run-sweep kernel (part of ms_pairs) */
 } tos_xi_stats;
 
 /* Opaque handles. */

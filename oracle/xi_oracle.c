@@ -18,7 +18,9 @@
  *  - SkyObject::angularSeparation (types.h:37-39) and XiBin::accumulate_pair
  *    (types.h:77-87): in mode 0 exactly as written (float products
  *    w*delta and wdi*wdj); in mode 1 ("FP64 oracle") every product and sum in
- *    double from the float inputs;
+ *    double from the float inputs; mode 2 is mode 1 with the absolute value
+ *    of every signed term (didj, di, dj), the scale against which a bin whose
+ *    signed sum cancels is judged;
  *  - HealpixBins::ang2pix (HealpixBins.h:58-72) with RING numbering
  *    (Gorski et al. 2005) for the cell of each sightline;
  *  - the brute-force estimator's histogram (gpu/brute.cu:40-52) with the FP64

@@ -58,6 +58,7 @@ __global__ void k_prep(const tos_pixel* raw, const uint64_t* off, const uint32_t
     double c0 = 0, c1 = 0, c2 = 0;
     float dmin = INFINITY, dmax = -INFINITY, lmin = INFINITY, lmax = -INFINITY;
     double mwd = 0, mw = 0, ml = 0, md = 0;
+    float gap = INFINITY;  // smallest positive step between consecutive distances
     bool unsorted = false;
     if (lane == 0) pre[0] = make_double4(0, 0, 0, 0);
     for (uint32_t b = 0; b < n; b += 32) {
@@ -86,6 +87,7 @@ __global__ void k_prep(const tos_pixel* raw, const uint64_t* off, const uint32_t
         if (k + 1 < n) {
           const tos_pixel nx = raw[o + k + 1];
           if (!(nx.distance >= px.distance) || !(nx.loglam >= px.loglam)) unsorted = true;
+          if (nx.distance > px.distance) gap = fminf(gap, __fsub_rd(nx.distance, px.distance));
         }
       }
       // inclusive warp scan, in order, of the three sums
@@ -114,11 +116,18 @@ __global__ void k_prep(const tos_pixel* raw, const uint64_t* off, const uint32_t
       mw = fmax(mw, __shfl_xor_sync(kFull, mw, d));
       ml = fmax(ml, __shfl_xor_sync(kFull, ml, d));
       md = fmax(md, __shfl_xor_sync(kFull, md, d));
+      gap = fminf(gap, __shfl_xor_sync(kFull, gap, d));
     }
     unsorted = __any_sync(kFull, unsorted);
     if (lane == 0) {
       range[s] = make_float4(dmin, dmax, lmin, lmax);
       if (unsorted) atomicOr(flags, 1u);
+      if (n > 0) {
+        // order key of a float: unsigned comparison of keys = float comparison
+        const unsigned u = __float_as_uint(dmin);
+        atomicMin(&flags[1], (u & 0x80000000u) ? ~u : (u | 0x80000000u));
+      }
+      atomicMin(&flags[2], __float_as_uint(gap));  // non-negative: bits order like values
       // non-negative doubles order like their bit patterns
       atomicMax(&maxbits[0], (unsigned long long)__double_as_longlong(mwd));
       atomicMax(&maxbits[1], (unsigned long long)__double_as_longlong(mw));
@@ -237,6 +246,19 @@ __global__ void k_expand(const uint32_t* members, uint32_t n_members, const uint
 // Per bin: convert every cell's 128-bit fixed-point sums to double and add
 // them in ascending cell order (the order of xi_finalize_task,
 // XiEstimator.cc:298-305).
+// Signed 128-bit fixed-point value {lo, hi} as a double with one relative
+// rounding: the magnitude is converted, so a small negative value (hi = -1,
+// lo close to 2^64) loses no low bits to the rounding of lo.
+__device__ __forceinline__ double i128_to_double(unsigned long long lo, long long hi) {
+  const bool neg = hi < 0;
+  if (neg) {
+    lo = ~lo + 1ull;
+    hi = (long long)(~(unsigned long long)hi + (lo == 0ull ? 1ull : 0ull));
+  }
+  const double m = __fma_rn((double)hi, 18446744073709551616.0 /* 2^64 */, (double)lo);
+  return neg ? -m : m;
+}
+
 __global__ void k_combine(const unsigned long long* acc, uint32_t n_cells, uint32_t nb,
                           double4 inv_a, double4 inv_b, tos_xibin* out, tos_xibin* cells_out) {
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
@@ -248,8 +270,7 @@ __global__ void k_combine(const unsigned long long* acc, uint32_t n_cells, uint3
       double v[7];
 #pragma unroll
       for (int k = 0; k < 7; ++k) {
-        // value = hi * 2^64 + lo (lo unsigned)
-        v[k] = __fma_rn((double)(long long)a[7 + k], 18446744073709551616.0, (double)a[k]) * inv[k];
+        v[k] = i128_to_double(a[k], (long long)a[7 + k]) * inv[k];
         s[k] += v[k];
       }
       n += (long long)a[14];
@@ -298,26 +319,34 @@ struct DeviceGuard {
   }
 };
 
-// Smallest float r >= 0 with ref_u32((r - min) * inv) >= n: every
-// |fl32(x1 - x2)| >= r is rejected by the first-axis check.
-float first_axis_limit(double min, double inv, uint32_t n) {
-  auto rejected = [&](float r) { return ref_u32(dmul(dsub((double)r, min), inv)) >= n; };
-  float hi = (float)(min + (double)n / inv);
-  if (!(hi > 0)) hi = 1.0f;
+// First-axis bin of a float separation r >= 0 as the reference decides it
+// (XiEstimator.cc:243, 280): -1 below the axis (t <= -1, where ref_u32 wraps),
+// the bin, or n above the axis.  Non-decreasing in r.
+int first_axis_code(float r, double min, double inv, uint32_t n) {
+  const double t = dmul(dsub((double)r, min), inv);
+  if (!(t > -1.0)) return -1;
+  if (t >= (double)n) return (int)n;
+  return (int)ref_u32(t);
+}
+
+// Smallest float r >= 0 whose first-axis code is >= k (k = 0..n); +inf when
+// there is none.  T[0] is the first accepted separation, T[k] <= r < T[k+1]
+// is bin k, and every |fl32(x1 - x2)| >= T[n] is rejected.
+float first_axis_threshold(double min, double inv, uint32_t n, int k) {
+  auto reached = [&](float r) { return first_axis_code(r, min, inv, n) >= k; };
+  if (reached(0.0f)) return 0.0f;
+  float hi = (float)std::max(1.0, min + (double)k / inv);
   int guard = 0;
-  while (!rejected(hi) && guard++ < 200) hi = hi * 2.0f + 1.0f;
-  if (!rejected(hi)) return INFINITY;
-  float lo = 0.0f;
-  if (rejected(lo)) return 0.0f;
-  // bisection over the ordered float bit patterns (both non-negative)
-  uint32_t a, b;
-  std::memcpy(&a, &lo, 4);
+  while (!reached(hi) && guard++ < 200) hi = hi * 2.0f + 1.0f;
+  if (!reached(hi)) return INFINITY;
+  // bisection over the ordered bit patterns of non-negative floats
+  uint32_t a = 0, b;
   std::memcpy(&b, &hi, 4);
   while (b - a > 1) {
     const uint32_t m = a + (b - a) / 2;
     float fm;
     std::memcpy(&fm, &m, 4);
-    if (rejected(fm))
+    if (reached(fm))
       b = m;
     else
       a = m;
@@ -525,7 +554,7 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
   TOS_TRY(cat->d_w.alloc(total));
   TOS_TRY(cat->d_prefix.alloc(total + n_los));
   TOS_TRY(cat->d_range.alloc(n_los));
-  TOS_TRY(cat->d_flags.alloc(1));
+  TOS_TRY(cat->d_flags.alloc(3));
   TOS_TRY(cat->d_maxes.alloc(4));
   cudaStream_t st = e->stream;
   TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_trig.p, trig.data(), n_los * sizeof(double4),
@@ -554,7 +583,10 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
                                        cudaMemcpyHostToDevice, st));
     }
   }
-  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_flags.p, 0, sizeof(unsigned int), st));
+  {
+    const unsigned int init[3] = {0u, 0xFFFFFFFFu, 0x7F800000u /* +inf */};
+    TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_flags.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  }
   TOS_CUDA_TRY(cudaMemsetAsync(cat->d_maxes.p, 0, 4 * sizeof(double), st));
   k_fill<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_dist_pad.p, padded, kSentinel);
   k_fill<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_loglam_pad.p, padded, kSentinel);
@@ -563,12 +595,22 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
       cat->d_wd.p, cat->d_w.p, cat->d_prefix.p, cat->d_range.p, cat->d_flags.p,
       (unsigned long long*)cat->d_maxes.p);
   TOS_CUDA_TRY(cudaGetLastError());
-  unsigned int flags = 0;
+  unsigned int fl[3] = {0u, 0u, 0u};
   double maxes[4];
-  TOS_CUDA_TRY(cudaMemcpyAsync(&flags, cat->d_flags.p, 4, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(fl, cat->d_flags.p, sizeof(fl), cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaMemcpyAsync(maxes, cat->d_maxes.p, 32, cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  const unsigned int flags = fl[0];
   cat->sorted = (flags & 1u) == 0;
+  {
+    const unsigned int key = fl[1];
+    const unsigned int u = (key & 0x80000000u) ? (key & 0x7FFFFFFFu) : ~key;
+    float f;
+    std::memcpy(&f, &u, 4);
+    cat->min_d = (total > 0) ? (double)f : 0.0;
+    std::memcpy(&f, &fl[2], 4);
+    cat->min_gap = (double)f;
+  }
   cat->max_abs_wd = maxes[0];
   cat->max_w = maxes[1];
   cat->max_l = maxes[2];
@@ -684,13 +726,16 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   TOS_TRY(cat->d_counters.alloc(4200));
   TOS_CUDA_TRY(cudaMemsetAsync(cat->d_cell_pairs.p, 0, nc * 8, st));
   TOS_CUDA_TRY(cudaMemsetAsync(cat->d_counters.p, 0, 4200 * 8, st));
-  unsigned long long* ctr = cat->d_counters.p;  // [0..3] pair kernel, [4] item counter, [8..] sep flags
+  // [0..3] kernel counters, [4] pair-kernel item counter, [5] candidates,
+  // [6] window flushes, [7] run-kernel item counter, [8] run items,
+  // [16] theta indices on an edge, [17..] their item numbers (4096 at most)
+  unsigned long long* ctr = cat->d_counters.p;
   const double theta_min = G.axis[1].min, theta_inv = 1.0 / axis_width(G.axis[1]);
   const int ge = grid_for(e, (size_t)nm * 32, 256);
   k_expand<<<ge, 256, 0, st>>>(cat->d_members.p, nm, cat->d_cell_idx.p, cat->d_cell_start.p,
                                cat->d_nb_start.p, cat->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
                                cat->d_cnt.p, cat->d_cand.p, cat->d_cell_pairs.p, nullptr, nullptr,
-                               nullptr, nullptr, nullptr, G.type, theta_min, theta_inv, ctr + 8);
+                               nullptr, nullptr, nullptr, G.type, theta_min, theta_inv, ctr + 16);
   TOS_CUDA_TRY(cudaGetLastError());
   // exclusive scan of counts -> item offsets
   size_t tmp_bytes = 0;
@@ -732,18 +777,18 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
                                cat->d_nb_start.p, cat->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
                                cat->d_cnt.p, cat->d_cand.p, cat->d_cell_pairs.p, cat->d_item_off.p,
                                cat->d_item_i.p, cat->d_item_j.p, cat->d_item_c.p,
-                               cat->d_item_sep.p, G.type, theta_min, theta_inv, ctr + 8);
+                               cat->d_item_sep.p, G.type, theta_min, theta_inv, ctr + 16);
   TOS_CUDA_TRY(cudaGetLastError());
   if (G.type == TOS_OBSERVING) {
     // theta indices within 1e-9 of an edge: recompute with the host libm acos,
     // the function the reference calls (XiEstimator.cc:166).
     unsigned long long nflag = 0;
-    TOS_CUDA_TRY(cudaMemcpyAsync(&nflag, ctr + 8, 8, cudaMemcpyDeviceToHost, st));
+    TOS_CUDA_TRY(cudaMemcpyAsync(&nflag, ctr + 16, 8, cudaMemcpyDeviceToHost, st));
     TOS_CUDA_TRY(cudaStreamSynchronize(st));
     if (nflag > 4096) return fail(TOS_ERR_UNSUPPORTED, "too many theta indices on a bin edge");
     if (nflag) {
       std::vector<unsigned long long> at(nflag);
-      TOS_CUDA_TRY(cudaMemcpy(at.data(), ctr + 9, nflag * 8, cudaMemcpyDeviceToHost));
+      TOS_CUDA_TRY(cudaMemcpy(at.data(), ctr + 17, nflag * 8, cudaMemcpyDeviceToHost));
       for (auto a : at) {
         double c;
         TOS_CUDA_TRY(cudaMemcpy(&c, cat->d_item_c.p + a, 8, cudaMemcpyDeviceToHost));
@@ -834,7 +879,7 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
       const double dm = cat->max_d;
       lim = (float)(std::sqrt(R * R + std::ldexp(dm * dm, -23) + 1e-3) * (1.0 + 1e-6) + 1e-3);
     } else {
-      lim = first_axis_limit(rg.min0, rg.inv0, n0);
+      lim = first_axis_threshold(rg.min0, rg.inv0, n0, (int)n0);
     }
     A.win_lim = lim;
     if (!std::isfinite(lim)) A.prune = 0;
@@ -854,14 +899,83 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
       A.win_slots = (int)std::min<uint32_t>(n0, (uint32_t)budget);
     }
   }
+  // --- run sweep (Cartesian and observing coordinates, sorted sightlines).
+  // The first-axis bin of |fl32(x1 - x2)| is decided by the exact float
+  // thresholds T[k]; for Cartesian coordinates r_perp must also be a
+  // non-decreasing function of the column distance along every row, as the
+  // reference computes it (XiEstimator.cc:244-248):
+  //   Y(d2) = fl(fl(r1_sq + fl(fl(d2 - tc) * d2)) - r_para^2)
+  //         = S * d2 - err + N,  S = 2 d1 - tc >= d1 (a - 2^-52), a = 2(1 - c),
+  // where err = d1^2 - fl32(d1^2) (|err| <= 2^-24 D^2) and the FP64 rounding
+  // |N| <= 11 * 2^-53 D^2 < 2^-49 D^2 (D the largest distance), provided
+  // fl32(d1 - d2) is exact (Sterbenz: |d1 - d2| < T[n0] <= d_min).  Then
+  //   (1) two columns at least `gap` apart differ in Y by S * gap - 2 |N| > 0
+  //       when a > 2^-52 + 2^-48 D^2 / (d_min * gap)   (per item: run_amin);
+  //   (2) Y >= -E with E = (2^-24 + 2^-49) D^2, and every |Y| <= E falls into
+  //       the r_perp code of 0 when the grid puts 0 and E in the same code,
+  // so the code of |Y| is non-decreasing along the row.
+  bool use_runs = false;
+  if (G.type != TOS_POLAR && cat->sorted && !A.force_exact && n_items > 0) {
+    std::vector<float> thr(n0 + 1);
+    for (uint32_t k = 0; k <= n0; ++k)
+      thr[k] = first_axis_threshold(rg.min0, rg.inv0, n0, (int)k);
+    use_runs = true;
+    A.run_amin = -1.0;
+    if (G.type == TOS_CARTESIAN) {
+      const double D = cat->max_d, dmin = cat->min_d, gap = cat->min_gap;
+      auto perp_code = [&](double x) {
+        const double t = tos::dmul(tos::dsub(std::sqrt(x), rg.min1), rg.inv1);
+        if (!(t > -1.0)) return -1;
+        return t >= (double)rg.n1 ? (int)rg.n1 : (int)ref_u32(t);
+      };
+      const double E = (std::ldexp(1.0, -24) + std::ldexp(1.0, -49)) * D * D * (1.0 + 1e-6);
+      if (!(dmin > 0) || !std::isfinite(thr[n0]) || !((double)thr[n0] * (1.0 + 1e-6) <= dmin) ||
+          perp_code(0.0) != perp_code(E) || !(gap > 0)) {
+        use_runs = false;
+      } else {
+        A.run_amin = std::isfinite(gap)
+                         ? (std::ldexp(1.0, -52) + std::ldexp(D * D, -48) / (dmin * gap)) * (1.0 + 1e-3)
+                         : std::ldexp(1.0, -51);
+      }
+    }
+    if (use_runs) {
+      TOS_TRY(cat->d_thr.alloc(n0 + 1));
+      TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_thr.p, thr.data(), (n0 + 1) * sizeof(float),
+                                   cudaMemcpyHostToDevice, st));
+      A.thr = cat->d_thr.p;
+      // one FP64 register sum can hold a whole item's pairs of a bin
+      // (at most max_np^2): every field takes the wide 62-bit conversion
+      const double m = std::max<double>(1.0, cat->max_np);
+      const double wdm = std::max(cat->max_abs_wd, 1e-300), wm = std::max(cat->max_w, 1e-300),
+                   lm = std::max(cat->max_l, 1e-300);
+      const double bound[7] = {wdm * m * wdm, wdm * m, m * wdm, wm * m * wm, wm * m, m * wm, lm * m};
+      for (int k = 0; k < 7; ++k) {
+        int f = (int)std::floor(62.0 - std::log2(bound[k] * m));
+        f = std::max(-60, std::min(f, 200));
+        A.scale[k] = std::ldexp(1.0, f);
+        A.scale_hi[k] = std::ldexp(1.0, f - 44);
+      }
+      A.wide_all = 1;
+      A.run_split = 1;
+    }
+  }
   if (n_items > 0) {
     TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    if (use_runs) {
+      PairArgs R = A;
+      R.next_item = ctr + 7;
+      const cudaError_t re = launch_run_kernel(R, G.type, minpos, e->num_sms, st);
+      if (re != cudaSuccess)
+        return fail(TOS_ERR_CUDA, std::string("run kernel: ") + cudaGetErrorString(re));
+    }
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
     const cudaError_t le =
         launch_pair_kernel(A, G.type, exact0, minpos, e->num_sms, st);
     if (le != cudaSuccess) return fail(TOS_ERR_CUDA, std::string("pair kernel: ") + cudaGetErrorString(le));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[3], st));
   } else {
     TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[3], st));
   }
   // --- combine cells
@@ -878,8 +992,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   if (want_cells)
     TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, cat->d_out.p + nb, (size_t)nc * nb * sizeof(tos_xibin),
                                  cudaMemcpyDeviceToHost, st));
-  unsigned long long hc[8];
-  TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, 64, cudaMemcpyDeviceToHost, st));
+  unsigned long long hc[9];
+  TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
   if (stats) {
@@ -907,6 +1021,9 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
     stats->ms_pairs = ms;
     cudaEventElapsedTime(&ms, e->ev[0], e->ev[4]);
     stats->ms_device = ms;
+    cudaEventElapsedTime(&ms, e->ev[2], e->ev[5]);
+    stats->ms_runs = ms;
+    stats->num_run_items = hc[8];
     stats->ms_total =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   }

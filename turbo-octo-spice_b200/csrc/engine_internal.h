@@ -94,10 +94,15 @@ struct tos_catalog {
   tos::DevBuf<float> d_w;           // weight per pixel
   tos::DevBuf<double4> d_prefix;    // per sightline N+1 exclusive prefix sums of (w*delta, w, loglam)
   tos::DevBuf<float4> d_range;      // per sightline (dmin, dmax, lmin, lmax)
-  tos::DevBuf<unsigned int> d_flags;// [0]: 1 if some sightline is not sorted by distance/loglam
+  tos::DevBuf<unsigned int> d_flags;// [0]: bit 0 some sightline is not sorted by distance and
+                                    // loglam, bit 1 a non-finite value; [1] order key of the
+                                    // smallest distance; [2] smallest positive gap between
+                                    // consecutive distances of a sightline (float bits)
   tos::DevBuf<double> d_maxes;      // [0] max|wd|, [1] max w, [2] max |loglam|, [3] max distance
   bool sorted = true;
   double max_abs_wd = 0, max_w = 0, max_l = 0, max_d = 0;
+  double min_d = 0;                 // smallest distance
+  double min_gap = 0;               // smallest positive distance step within a sightline (lower bound)
   uint32_t max_np = 0;
   // run scratch (kept between runs)
   tos::DevBuf<uint32_t> d_nb_count, d_nb_start, d_nb;  // cell neighbour CSR
@@ -110,5 +115,6 @@ struct tos_catalog {
   tos::DevBuf<unsigned long long> d_acc;               // [n_cells][n_bins][16] 128-bit fixed point
   tos::DevBuf<tos_xibin> d_out;                        // combined / per cell output
   tos::DevBuf<unsigned long long> d_counters;          // misc counters
+  tos::DevBuf<float> d_thr;                            // first-axis thresholds of the run sweep
   tos::DevBuf<unsigned char> d_cub_tmp;
 };

@@ -1,0 +1,111 @@
+// xi_device.cuh — device helpers shared by the pixel-pair kernel
+// (xi_kernels.cu) and the run-sweep kernel (xi_runs.cu): FP32 approximations,
+// fixed-point conversion, 128-bit accumulation, and the exact re-binning that
+// follows the reference's FP64 expression order.
+#pragma once
+
+#include "xi_kernels.cuh"
+
+namespace tos {
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+enum { kPolar = TOS_POLAR, kCart = TOS_CARTESIAN, kObs = TOS_OBSERVING };
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Fixed-point image round(c * scale) of a contribution, |c*scale| < 2^51.
+__device__ __forceinline__ long long to_fixed(double c, double scale) {
+  return __double_as_longlong(__fma_rn(c, scale, kMagic52)) - kMagic52Bits;
+}
+
+// round(c * 2^F) for |c * 2^F| < 2^62, given sh = 2^(F-44): the high part is
+// rounded first and the exact remainder carries the low 44 bits.
+__device__ __forceinline__ long long to_fixed_wide(double c, double sh) {
+  const double v = c * sh;
+  const long long qh = __double_as_longlong(__dadd_rn(v, kMagic52)) - kMagic52Bits;
+  const double rem = v - (double)qh;  // exact, |rem| <= 0.5
+  return (qh << 44) + to_fixed(rem, 17592186044416.0 /* 2^44 */);
+}
+
+// Window word of field k, part p (0 = low).
+__device__ __forceinline__ int wword(int k, int p) {
+  return (k < kSigned) ? 3 * k + p : 3 * kSigned + 2 * (k - kSigned) + p;
+}
+constexpr int kWordCount = 3 * kSigned + 2 * (7 - kSigned);      // 17
+constexpr int kWordContrib = kWordCount + 1;                     // 18
+
+// Add a signed 64-bit value to a 128-bit accumulator {lo: u64, hi: i64}.
+__device__ __forceinline__ void add128(unsigned long long* lo, unsigned long long* hi, long long q) {
+  const unsigned long long uq = (unsigned long long)q;
+  const unsigned long long old = atomicAdd(lo, uq);
+  const long long carry = (old + uq < old) ? 1 : 0;
+  const long long h = (q < 0 ? -1 : 0) + carry;
+  if (h != 0) atomicAdd(hi, (unsigned long long)h);
+}
+
+// ---- exact re-binning (reference expression order) returning the two axis
+// indices; z is handled per item.  Mirrors ref_bin_* in tos_common.h.
+__device__ __forceinline__ bool exact_cart(float d1, float d2, double c, const RefGrid& g,
+                                           uint32_t* b0, uint32_t* b1) {
+  const double r1_sq = (double)fmul(d1, d1);
+  const double two_r1_cos12 = dmul((double)fmul(2.0f, d1), c);
+  const double r_para = (double)fabsf(fsub(d1, d2));
+  const uint32_t p = ref_u32(dmul(dsub(r_para, g.min0), g.inv0));
+  if (p >= g.n0) return false;
+  const double r_sq = dadd(r1_sq, dmul(dsub((double)d2, two_r1_cos12), (double)d2));
+  const double x = fabs(dsub(r_sq, dmul(r_para, r_para)));
+  const uint32_t q = ref_u32(dmul(dsub(dsqrt(x), g.min1), g.inv1));
+  if (q >= g.n1) return false;
+  *b0 = p;
+  *b1 = q;
+  return true;
+}
+
+__device__ __forceinline__ bool exact_polar(float d1, float d2, double c, const RefGrid& g,
+                                            uint32_t* b0, uint32_t* b1) {
+  const double r1_sq = (double)fmul(d1, d1);
+  const double two_r1_cos12 = dmul((double)fmul(2.0f, d1), c);
+  const double r_sq = dadd(r1_sq, dmul(dsub((double)d2, two_r1_cos12), (double)d2));
+  const double r = dsqrt(r_sq);
+  const uint32_t p = ref_u32(dmul(dsub(r, g.min0), g.inv0));
+  if (p >= g.n0) return false;
+  if (r == 0) return false;
+  const double mu = ddiv((double)fabsf(fsub(d1, d2)), r);
+  const uint32_t q = ref_u32(dmul(dsub(mu, g.min1), g.inv1));
+  if (q >= g.n1) return false;
+  *b0 = p;
+  *b1 = q;
+  return true;
+}
+
+__device__ __forceinline__ bool exact_obs(float l1, float l2, const RefGrid& g, uint32_t* b0) {
+  const uint32_t p = ref_u32(dmul(dsub((double)fabsf(fsub(l1, l2)), g.min0), g.inv0));
+  if (p >= g.n0) return false;
+  *b0 = p;
+  return true;
+}
+
+// Items of the run-sweep kernel when A.run_split is set: z index constant
+// over the item and (Cartesian) 2(1 - cos theta) large enough for the
+// reference's r_perp expression to grow with the column distance along every
+// row.  Both kernels evaluate this same predicate.
+__device__ __forceinline__ bool run_item(const PairArgs& A, double c, bool zconst) {
+  return zconst && dmul(2.0, dsub(1.0, c)) >= A.run_amin;
+}
+
+__device__ __forceinline__ uint32_t zbin_of_sum(float lsum, const RefGrid& g) {
+  return ref_u32(dmul(dsub(dmul(0.5, (double)lsum), g.min2), g.invn2));
+}
+
+}  // namespace
+}  // namespace tos

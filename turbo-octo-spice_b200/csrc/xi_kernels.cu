@@ -1,99 +1,10 @@
 // xi_kernels.cu — the persistent pixel-pair kernel (see xi_kernels.cuh).
 #include "xi_kernels.cuh"
+#include "xi_device.cuh"
 
 namespace tos {
 
 namespace {
-
-constexpr unsigned kFull = 0xFFFFFFFFu;
-enum { kPolar = TOS_POLAR, kCart = TOS_CARTESIAN, kObs = TOS_OBSERVING };
-
-__device__ __forceinline__ float sqrt_approx(float x) {
-  float r;
-  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
-__device__ __forceinline__ float rsqrt_approx(float x) {
-  float r;
-  asm("rsqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
-
-// Fixed-point image round(c * scale) of a contribution, |c*scale| < 2^51.
-__device__ __forceinline__ long long to_fixed(double c, double scale) {
-  return __double_as_longlong(__fma_rn(c, scale, kMagic52)) - kMagic52Bits;
-}
-
-// round(c * 2^F) for |c * 2^F| < 2^62, given sh = 2^(F-44): the high part is
-// rounded first and the exact remainder carries the low 44 bits.
-__device__ __forceinline__ long long to_fixed_wide(double c, double sh) {
-  const double v = c * sh;
-  const long long qh = __double_as_longlong(__dadd_rn(v, kMagic52)) - kMagic52Bits;
-  const double rem = v - (double)qh;  // exact, |rem| <= 0.5
-  return (qh << 44) + to_fixed(rem, 17592186044416.0 /* 2^44 */);
-}
-
-// Window word of field k, part p (0 = low).
-__device__ __forceinline__ int wword(int k, int p) {
-  return (k < kSigned) ? 3 * k + p : 3 * kSigned + 2 * (k - kSigned) + p;
-}
-constexpr int kWordCount = 3 * kSigned + 2 * (7 - kSigned);      // 17
-constexpr int kWordContrib = kWordCount + 1;                     // 18
-
-// Add a signed 64-bit value to a 128-bit accumulator {lo: u64, hi: i64}.
-__device__ __forceinline__ void add128(unsigned long long* lo, unsigned long long* hi, long long q) {
-  const unsigned long long uq = (unsigned long long)q;
-  const unsigned long long old = atomicAdd(lo, uq);
-  const long long carry = (old + uq < old) ? 1 : 0;
-  const long long h = (q < 0 ? -1 : 0) + carry;
-  if (h != 0) atomicAdd(hi, (unsigned long long)h);
-}
-
-// ---- exact re-binning (reference expression order) returning the two axis
-// indices; z is handled per item.  Mirrors ref_bin_* in tos_common.h.
-__device__ __forceinline__ bool exact_cart(float d1, float d2, double c, const RefGrid& g,
-                                           uint32_t* b0, uint32_t* b1) {
-  const double r1_sq = (double)fmul(d1, d1);
-  const double two_r1_cos12 = dmul((double)fmul(2.0f, d1), c);
-  const double r_para = (double)fabsf(fsub(d1, d2));
-  const uint32_t p = ref_u32(dmul(dsub(r_para, g.min0), g.inv0));
-  if (p >= g.n0) return false;
-  const double r_sq = dadd(r1_sq, dmul(dsub((double)d2, two_r1_cos12), (double)d2));
-  const double x = fabs(dsub(r_sq, dmul(r_para, r_para)));
-  const uint32_t q = ref_u32(dmul(dsub(dsqrt(x), g.min1), g.inv1));
-  if (q >= g.n1) return false;
-  *b0 = p;
-  *b1 = q;
-  return true;
-}
-
-__device__ __forceinline__ bool exact_polar(float d1, float d2, double c, const RefGrid& g,
-                                            uint32_t* b0, uint32_t* b1) {
-  const double r1_sq = (double)fmul(d1, d1);
-  const double two_r1_cos12 = dmul((double)fmul(2.0f, d1), c);
-  const double r_sq = dadd(r1_sq, dmul(dsub((double)d2, two_r1_cos12), (double)d2));
-  const double r = dsqrt(r_sq);
-  const uint32_t p = ref_u32(dmul(dsub(r, g.min0), g.inv0));
-  if (p >= g.n0) return false;
-  if (r == 0) return false;
-  const double mu = ddiv((double)fabsf(fsub(d1, d2)), r);
-  const uint32_t q = ref_u32(dmul(dsub(mu, g.min1), g.inv1));
-  if (q >= g.n1) return false;
-  *b0 = p;
-  *b1 = q;
-  return true;
-}
-
-__device__ __forceinline__ bool exact_obs(float l1, float l2, const RefGrid& g, uint32_t* b0) {
-  const uint32_t p = ref_u32(dmul(dsub((double)fabsf(fsub(l1, l2)), g.min0), g.inv0));
-  if (p >= g.n0) return false;
-  *b0 = p;
-  return true;
-}
-
-__device__ __forceinline__ uint32_t zbin_of_sum(float lsum, const RefGrid& g) {
-  return ref_u32(dmul(dsub(dmul(0.5, (double)lsum), g.min2), g.invn2));
-}
 
 // Per-row (lane) state of a chunk.
 struct Row {
@@ -159,7 +70,8 @@ __device__ void add_direct(const PairArgs& A, uint32_t cell, uint32_t idx, const
 #pragma unroll
   for (int k = 0; k < 7; ++k)
     add128(base + k, base + 7 + k,
-           k < kSigned ? to_fixed_wide(c[k], A.scale_hi[k]) : to_fixed(c[k], A.scale[k]));
+           (k < kSigned || A.wide_all) ? to_fixed_wide(c[k], A.scale_hi[k])
+                                       : to_fixed(c[k], A.scale[k]));
   atomicAdd(base + 14, (unsigned long long)m);
   atomicAdd(&A.counters[3], 1ull);
 }
@@ -571,7 +483,10 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) pair_kernel(PairArgs A) {
     it.zb = zbin_of_sum(lsum_lo, A.g);
     it.zconst = (zlo > -1.0 && zhi < 2147483648.0 && it.zb == zbin_of_sum(lsum_hi, A.g)) ? 1 : 0;
     it.lo1 = 0;
-    const bool exact_item = A.force_exact || !it.zconst;
+    if (A.run_split && run_item(A, it.c, it.zconst)) continue;  // run-sweep kernel's item
+    // with run_split every field uses the wide fixed-point scale, which only
+    // the direct (exact) path supports
+    const bool exact_item = A.force_exact || !it.zconst || A.run_split;
     if (exact_item)
       process_item<COORD, EXACT0, MINPOS, 1>(A, it, win, lane, n_eval, n_recheck);
     else

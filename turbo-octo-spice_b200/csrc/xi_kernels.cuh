@@ -77,18 +77,29 @@ struct PairArgs {
   int prune;                 // sightlines sorted: restrict columns to the r_par window
   // accumulation
   double scale[7];           // 2^F per field
-  double scale_hi[3];        // 2^(F-44) for the signed fields
+  double scale_hi[7];        // 2^(F-44): wide (62-bit) conversion of a field
+  int wide_all;              // every field uses the wide conversion (direct adds only)
+  int run_split;             // the run-sweep kernel takes the items run_item() accepts; the
+                             // pixel-pair kernel skips those and evaluates the rest exactly
+  double run_amin;           // Cartesian: smallest 2(1 - cos theta) the run sweep accepts
+  const float* thr;          // run sweep: first-axis thresholds T[0..n0]
   int win_w1;                // window width along axis 1 (Cartesian)
   int win_slots;             // slots per warp window
   unsigned long long* acc;   // [n_cells][ntotal][kAccWords] 128-bit fixed point
   unsigned long long* counters;  // [0] evaluated pairs [1] rechecks [2] overflow pairs
-                                 // [3] direct runs [4] item counter [6] window flushes
+                                 // [3] direct runs [6] window flushes
   int force_exact;           // evaluate every pixel pair with the FP64 reference
 };
 
-// Launch the persistent pair kernel (coordinate type from a.g/a.* fields).
+// Launch the persistent pixel-pair kernel (coordinate type from a.g/a.* fields).
 cudaError_t launch_pair_kernel(const PairArgs& a, int coord, bool exact0, bool minpos, int grid,
                                cudaStream_t stream);
 size_t pair_kernel_smem(int win_slots);
+
+// Launch the persistent run-sweep kernel (xi_runs.cu) over the items that
+// run_item() accepts: Cartesian and observing coordinates, catalogue sorted
+// by distance and loglam, a.thr set and every field on the wide scale.
+cudaError_t launch_run_kernel(const PairArgs& a, int coord, bool minpos, int num_sms,
+                              cudaStream_t stream);
 
 }  // namespace tos
