@@ -112,8 +112,9 @@ typedef struct {
   double ms_pairs;                   /* device time: run-sweep and pixel-pair kernels */
   double ms_total;                   /* wall time of the call */
   double ms_device;                  /* device time of the whole call (expansion to results) */
-  uint64_t num_run_items;            /* sightline pairs counted by the run-sweep kernel */
-  double ms_runs;                    /* device time: run-sweep kernel (part of ms_pairs) */
+  uint64_t num_run_items;            /* sightline pairs counted by the boundary-sweep kernels */
+  double ms_runs;                    /* device time: grid- and run-sweep kernels (part of ms_pairs) */
+  uint64_t num_grid_items;           /* of num_run_items: sightline pairs counted by the grid-sweep kernel */
 } tos_xi_stats;
 
 /* Opaque handles. */

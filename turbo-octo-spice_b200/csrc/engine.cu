@@ -267,13 +267,16 @@ __global__ void k_combine(const unsigned long long* acc, uint32_t n_cells, uint3
     long long n = 0;
     for (uint32_t c = 0; c < n_cells; ++c) {
       const unsigned long long* a = acc + ((size_t)c * nb + b) * kAccWords;
+      // a bin without pairs has zero sums: the telescoped dipoles of its
+      // neighbours cancel in it only up to the rounding of their FP64 sums
+      const long long cnt = (long long)a[14];
       double v[7];
 #pragma unroll
       for (int k = 0; k < 7; ++k) {
-        v[k] = i128_to_double(a[k], (long long)a[7 + k]) * inv[k];
+        v[k] = (cnt != 0) ? i128_to_double(a[k], (long long)a[7 + k]) * inv[k] : 0.0;
         s[k] += v[k];
       }
-      n += (long long)a[14];
+      n += cnt;
       if (cells_out) {
         tos_xibin x;
         x.didj = v[0];
@@ -283,7 +286,7 @@ __global__ void k_combine(const unsigned long long* acc, uint32_t n_cells, uint3
         x.wi = v[4];
         x.wj = v[5];
         x.z = v[6];
-        x.num_pairs = (long long)a[14];
+        x.num_pairs = cnt;
         cells_out[(size_t)c * nb + b] = x;
       }
     }
@@ -404,6 +407,124 @@ double max_angular_scale(const tos_grid& g, double scale) {
 }  // namespace tos
 
 using namespace tos;
+
+// ---------------------------------------------------------------------------
+// Common first-axis grid of a catalogue (grid sweep, xi_grid.cu)
+// ---------------------------------------------------------------------------
+
+// One warp per sightline: grid index of pixel 0 when the sightline's values
+// are consecutive entries of the sorted distinct values U, else kNoGrid.
+__global__ void k_grid_first(const float* xpad, const uint64_t* off, const uint32_t* npix,
+                             size_t n_los, const float* U, int ng, uint32_t* gfirst,
+                             unsigned long long* n_ok) {
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t s = warp; s < n_los; s += nwarps) {
+    const uint32_t n = npix[s];
+    const float* x = xpad + off[s] + (uint64_t)kPad * (s + 1);
+    uint32_t f = kNoGrid;
+    if (n > 0) {
+      int lo = 0, hi = ng;  // first U >= x[0]
+      const float x0 = x[0];
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (U[mid] < x0)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      bool ok = (uint64_t)lo + n <= (uint64_t)ng;
+      for (uint32_t p = lane; ok && p < n; p += 32) ok = U[lo + p] == x[p];
+      ok = __all_sync(kFull, ok);
+      if (ok) f = (uint32_t)lo;
+    }
+    if (lane == 0) {
+      gfirst[s] = f;
+      if (f != kNoGrid) atomicAdd(n_ok, 1ull);
+    }
+  }
+}
+
+// Boundary table Q[side][g][k] = first grid index g2 whose value x2 = U[g2]
+// passes the boundary predicate of threshold T[k] against x1 = U[g]:
+//   side 0: x2 >= x1 and fl(x2 - x1) >= T[k];  side 1: x2 >= x1 or fl(x1 - x2) < T[k].
+__global__ void k_grid_table(const float* U, int ng, const float* thr, int nk, uint16_t* Q) {
+  const size_t total = (size_t)2 * ng * nk;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e % nk);
+    const int g = (int)((e / nk) % ng);
+    const int side = (int)(e / ((size_t)nk * ng));
+    const float x1 = U[g], t = thr[k];
+    int lo = 0, hi = ng;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      const float x2 = U[mid];
+      const bool ge = x2 >= x1;
+      const bool pass = side ? (ge || !(__fsub_rn(x1, x2) >= t)) : (ge && __fsub_rn(x2, x1) >= t);
+      if (pass)
+        hi = mid;
+      else
+        lo = mid + 1;
+    }
+    Q[e] = (uint16_t)lo;
+  }
+}
+
+// Build (once per catalogue and coordinate) the sorted distinct values of the
+// padded coordinate array and the per-sightline grid offsets.  Grids of more
+// than 65535 values are not used.
+tos_status ensure_grid(tos_engine* e, tos_catalog* cat, int w, cudaStream_t st) {
+  if (cat->grid_built[w]) return TOS_OK;
+  const float* x = (w == 0) ? cat->d_dist_pad.p : cat->d_loglam_pad.p;
+  const size_t n = (w == 0) ? cat->d_dist_pad.n : cat->d_loglam_pad.n;
+  if (n > (size_t)0x7FFFFFFF) {  // beyond the 32-bit item counts of the sort
+    cat->grid_built[w] = true;
+    cat->grid_n[w] = 0;
+    return TOS_OK;
+  }
+  DevBuf<float> sorted, uniq;
+  DevBuf<int> nsel;
+  TOS_TRY(sorted.alloc(n));
+  TOS_TRY(uniq.alloc(n));
+  TOS_TRY(nsel.alloc(1));
+  size_t tb1 = 0, tb2 = 0;
+  cub::DeviceRadixSort::SortKeys(nullptr, tb1, x, sorted.p, (int)n, 0, 32, st);
+  cub::DeviceSelect::Unique(nullptr, tb2, sorted.p, uniq.p, nsel.p, (int)n, st);
+  DevBuf<unsigned char> tmp;
+  TOS_TRY(tmp.alloc(std::max(tb1, tb2) + 16));
+  TOS_CUDA_TRY(cub::DeviceRadixSort::SortKeys(tmp.p, tb1, x, sorted.p, (int)n, 0, 32, st));
+  TOS_CUDA_TRY(cub::DeviceSelect::Unique(tmp.p, tb2, sorted.p, uniq.p, nsel.p, (int)n, st));
+  int ng = 0;
+  TOS_CUDA_TRY(cudaMemcpyAsync(&ng, nsel.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  // the padding sentinel is the largest value: not part of the grid
+  if (ng > 0) {
+    float last = 0;
+    TOS_CUDA_TRY(cudaMemcpy(&last, uniq.p + ng - 1, sizeof(float), cudaMemcpyDeviceToHost));
+    if (last == kSentinel) --ng;
+  }
+  cat->grid_built[w] = true;
+  cat->grid_n[w] = 0;
+  if (ng <= 0 || ng > 65535) return TOS_OK;
+  TOS_TRY(cat->d_grid[w].alloc(ng));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_grid[w].p, uniq.p, ng * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  TOS_TRY(cat->d_gfirst[w].alloc(cat->n_los));
+  TOS_CUDA_TRY(cudaMemsetAsync(nsel.p, 0, sizeof(int), st));
+  DevBuf<unsigned long long> nok;
+  TOS_TRY(nok.alloc(1));
+  TOS_CUDA_TRY(cudaMemsetAsync(nok.p, 0, 8, st));
+  k_grid_first<<<grid_for(e, cat->n_los * 32, 256), 256, 0, st>>>(
+      x, cat->d_off.p, cat->d_npix.p, cat->n_los, cat->d_grid[w].p, ng, cat->d_gfirst[w].p, nok.p);
+  TOS_CUDA_TRY(cudaGetLastError());
+  unsigned long long h = 0;
+  TOS_CUDA_TRY(cudaMemcpyAsync(&h, nok.p, 8, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  cat->grid_n[w] = ng;
+  cat->grid_los[w] = h;
+  return TOS_OK;
+}
 
 // ============================================================================
 // C ABI
@@ -727,7 +848,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   TOS_CUDA_TRY(cudaMemsetAsync(cat->d_cell_pairs.p, 0, nc * 8, st));
   TOS_CUDA_TRY(cudaMemsetAsync(cat->d_counters.p, 0, 4200 * 8, st));
   // [0..3] kernel counters, [4] pair-kernel item counter, [5] candidates,
-  // [6] window flushes, [7] run-kernel item counter, [8] run items,
+  // [6] window flushes, [7] run-kernel item counter, [8] run items, [9] grid
+  // items, [10] grid-kernel item counter,
   // [16] theta indices on an edge, [17..] their item numbers (4096 at most)
   unsigned long long* ctr = cat->d_counters.p;
   const double theta_min = G.axis[1].min, theta_inv = 1.0 / axis_width(G.axis[1]);
@@ -915,7 +1037,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   //       the r_perp code of 0 when the grid puts 0 and E in the same code,
   // so the code of |Y| is non-decreasing along the row.
   bool use_runs = false;
-  if (G.type != TOS_POLAR && cat->sorted && !A.force_exact && n_items > 0) {
+  // (per-lane pair counts are 32-bit: at most max_np^2 < 2^32 pairs per item)
+  if (G.type != TOS_POLAR && cat->sorted && !A.force_exact && n_items > 0 && cat->max_np < 65536) {
     std::vector<float> thr(n0 + 1);
     for (uint32_t k = 0; k <= n0; ++k)
       thr[k] = first_axis_threshold(rg.min0, rg.inv0, n0, (int)k);
@@ -930,6 +1053,7 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
       };
       const double E = (std::ldexp(1.0, -24) + std::ldexp(1.0, -49)) * D * D * (1.0 + 1e-6);
       if (!(dmin > 0) || !std::isfinite(thr[n0]) || !((double)thr[n0] * (1.0 + 1e-6) <= dmin) ||
+          !(D * rg.inv1 < 1e6) ||
           perp_code(0.0) != perp_code(E) || !(gap > 0)) {
         use_runs = false;
       } else {
@@ -959,8 +1083,34 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
       A.run_split = 1;
     }
   }
+  // --- grid sweep: catalogues whose first-axis values lie on a small common grid
+  bool use_grid = false;
+  if (use_runs) {
+    const int w = (G.type == TOS_OBSERVING) ? 1 : 0;
+    TOS_TRY(ensure_grid(e, cat, w, st));
+    const int ng = cat->grid_n[w];
+    if (ng > 0 && cat->grid_los[w] > 0) {
+      const size_t nq = (size_t)2 * ng * (n0 + 1);
+      TOS_TRY(cat->d_gq.alloc(nq));
+      k_grid_table<<<grid_for(e, nq, 256), 256, 0, st>>>(cat->d_grid[w].p, ng, cat->d_thr.p,
+                                                         (int)n0 + 1, cat->d_gq.p);
+      TOS_CUDA_TRY(cudaGetLastError());
+      A.gq = cat->d_gq.p;
+      A.gfirst = cat->d_gfirst[w].p;
+      A.ng = ng;
+      A.grid_split = 1;
+      use_grid = true;
+    }
+  }
   if (n_items > 0) {
     TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    if (use_grid) {
+      PairArgs R = A;
+      R.next_item = ctr + 10;
+      const cudaError_t ge2 = launch_grid_kernel(R, G.type, minpos, e->num_sms, st);
+      if (ge2 != cudaSuccess)
+        return fail(TOS_ERR_CUDA, std::string("grid kernel: ") + cudaGetErrorString(ge2));
+    }
     if (use_runs) {
       PairArgs R = A;
       R.next_item = ctr + 7;
@@ -992,7 +1142,7 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   if (want_cells)
     TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, cat->d_out.p + nb, (size_t)nc * nb * sizeof(tos_xibin),
                                  cudaMemcpyDeviceToHost, st));
-  unsigned long long hc[9];
+  unsigned long long hc[10];
   TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1023,7 +1173,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
     stats->ms_device = ms;
     cudaEventElapsedTime(&ms, e->ev[2], e->ev[5]);
     stats->ms_runs = ms;
-    stats->num_run_items = hc[8];
+    stats->num_run_items = hc[8] + hc[9];
+    stats->num_grid_items = hc[9];
     stats->ms_total =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   }

@@ -116,5 +116,12 @@ struct tos_catalog {
   tos::DevBuf<tos_xibin> d_out;                        // combined / per cell output
   tos::DevBuf<unsigned long long> d_counters;          // misc counters
   tos::DevBuf<float> d_thr;                            // first-axis thresholds of the run sweep
+  // common first-axis grids (0: distance, 1: loglam), built on first use
+  bool grid_built[2] = {false, false};
+  int grid_n[2] = {0, 0};                              // distinct values (0: no usable grid)
+  uint64_t grid_los[2] = {0, 0};                       // sightlines contiguous on the grid
+  tos::DevBuf<float> d_grid[2];                        // sorted distinct values
+  tos::DevBuf<uint32_t> d_gfirst[2];                   // per sightline grid index of pixel 0 or kNoGrid
+  tos::DevBuf<uint16_t> d_gq;                          // boundary table of the current call
   tos::DevBuf<unsigned char> d_cub_tmp;
 };

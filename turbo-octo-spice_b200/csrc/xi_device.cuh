@@ -103,6 +103,12 @@ __device__ __forceinline__ bool run_item(const PairArgs& A, double c, bool zcons
   return zconst && dmul(2.0, dsub(1.0, c)) >= A.run_amin;
 }
 
+// Run items whose sightlines are both contiguous on the common grid: the
+// grid-sweep kernel's share when A.grid_split is set.
+__device__ __forceinline__ bool grid_item(const PairArgs& A, uint32_t i, uint32_t j) {
+  return A.grid_split && A.gfirst[i] != kNoGrid && A.gfirst[j] != kNoGrid;
+}
+
 __device__ __forceinline__ uint32_t zbin_of_sum(float lsum, const RefGrid& g) {
   return ref_u32(dmul(dsub(dmul(0.5, (double)lsum), g.min2), g.invn2));
 }

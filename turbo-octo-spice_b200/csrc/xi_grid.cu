@@ -1,0 +1,112 @@
+// xi_grid.cu — grid-sweep kernel of the XiEstimator pair count (Cartesian
+// and observing coordinates) for catalogues whose first-axis coordinate takes
+// few distinct values: forests on a common log-wavelength grid, whose
+// distances are one function of loglam (h5healxi.cc:196-203).
+//
+// With U the sorted distinct first-axis values of the catalogue and a
+// sightline contiguous on U (its pixel p has value U[f + p]), the run
+// boundaries of xi_sweep.cuh for a row x1 = U[g] along any column sightline j
+// are
+//   q_k = clamp(Q[side][g][k] - f_j, 0, n_j),
+// where Q[side][g][k] is the first grid index g2 whose value passes the
+// boundary predicate of threshold T[k] against U[g].  Q is built once per
+// call (k_grid_table, engine.cu), so a lane reads both ends of its run with
+// two adjacent table loads instead of walking pointers.
+#include "xi_sweep.cuh"
+
+namespace tos {
+namespace {
+
+constexpr int kGridWarps = 4;  // warps per CTA of the grid-sweep kernel
+
+// Rows [r_lo, r_hi) of an item for the 32 (side, bin) tasks t0 + lane.
+template <int COORD, bool MINPOS>
+__device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, int fi, int fj,
+                                        int t0, int lane, unsigned long long* stats) {
+  const int n0 = (int)A.g.n0;
+  const int task = t0 + lane;
+  const bool act = task < 2 * n0;
+  const int side = act ? task / n0 : 0;
+  const int k = act ? task % n0 : 0;
+  const int nj = it.nj;
+  const size_t qstride = (size_t)(n0 + 1);
+  const uint16_t* qrow = A.gq + ((size_t)side * A.ng + fi) * qstride + k;
+  RunAcc acc;
+  acc.B = -1;
+#pragma unroll
+  for (int f = 0; f < 8; ++f) acc.s0[f] = acc.s1[f] = 0.0;
+  unsigned rech = 0;
+  unsigned long long n_eval = 0;
+  // boundaries loaded one row ahead
+  ushort2 nQ = make_ushort2(qrow[(size_t)it.r_lo * qstride], qrow[(size_t)it.r_lo * qstride + 1]);
+#pragma unroll 1
+  for (int r = it.r_lo; r < it.r_hi; ++r) {
+    const ushort2 Qv = nQ;
+    const int rn = min(r + 1, it.r_hi - 1);
+    nQ = make_ushort2(qrow[(size_t)rn * qstride], qrow[(size_t)rn * qstride + 1]);
+    const int qa = min(max((int)Qv.x - fj, 0), nj), qb = min(max((int)Qv.y - fj, 0), nj);
+    const int s = side ? qb : qa, e = side ? qa : qb;
+    if (act && e > s) {
+      n_eval += (unsigned long long)(e - s);
+      const RowV R = row_values<COORD>(A, it, r);
+      do_run<COORD, MINPOS>(A, it.d, it.colx, it.pre, it.c, R, k, s, e, acc, rech);
+    }
+  }
+  if (act) {
+    acc_flush8<COORD>(A, it.d, k, acc.B, acc.s0);
+    acc_flush8<COORD>(A, it.d, k, acc.B + 1, acc.s1);
+  }
+  stats[0] += n_eval;
+  stats[1] += rech;
+}
+
+template <int COORD, bool MINPOS>
+__global__ void __launch_bounds__(kGridWarps * 32, 4) grid_kernel(PairArgs args) {
+  // the arguments in shared memory: helpers take them by reference without a
+  // per-thread local copy of the parameter block
+  __shared__ PairArgs A;
+  if (threadIdx.x == 0) A = args;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  unsigned long long stats[2] = {0ull, 0ull};  // evaluated pairs, FP64 re-evaluations
+  unsigned long long n_taken = 0;
+  const int n0 = (int)A.g.n0;
+  const float tmax = A.thr[n0];  // fl|x1 - x2| >= tmax: rejected by the first axis
+  for (;;) {
+    unsigned long long idx = 0;
+    if (lane == 0) idx = atomicAdd(A.next_item, 1ull);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= A.n_items) break;
+    SweepItem it;
+    if (!load_item<COORD>(A, idx, tmax, it)) continue;  // another kernel's item
+    if (!grid_item(A, it.i, it.j)) continue;             // the pointer sweep's item
+    ++n_taken;
+    if (it.r_hi <= it.r_lo) continue;
+    const int fi = (int)A.gfirst[it.i], fj = (int)A.gfirst[it.j];
+    for (int t0 = 0; t0 < 2 * n0; t0 += 32) grid_group<COORD, MINPOS>(A, it, fi, fj, t0, lane, stats);
+  }
+  add_counters(A, lane, stats[0], stats[1], n_taken, 9);
+}
+
+// Persistent launch: as many CTAs as fit on the SMs at once.
+template <int COORD, bool MINPOS>
+cudaError_t launch_grid(const PairArgs& a, int num_sms, cudaStream_t stream) {
+  int per_sm = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, grid_kernel<COORD, MINPOS>, kGridWarps * 32, 0);
+  if (e != cudaSuccess) return e;
+  grid_kernel<COORD, MINPOS><<<num_sms * (per_sm > 0 ? per_sm : 1), kGridWarps * 32, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_grid_kernel(const PairArgs& a, int coord, bool minpos, int num_sms,
+                               cudaStream_t stream) {
+  if (coord == TOS_CARTESIAN)
+    return minpos ? launch_grid<kCart, true>(a, num_sms, stream)
+                  : launch_grid<kCart, false>(a, num_sms, stream);
+  return minpos ? launch_grid<kObs, true>(a, num_sms, stream) : launch_grid<kObs, false>(a, num_sms, stream);
+}
+
+}  // namespace tos

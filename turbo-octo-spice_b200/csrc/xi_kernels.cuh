@@ -33,6 +33,7 @@
 namespace tos {
 
 constexpr uint32_t kInvalidKey = 0xFFFFFFFFu;
+constexpr uint32_t kNoGrid = 0xFFFFFFFFu;  // sightline not contiguous on the common grid
 constexpr int kPairWarps = 12;  // warps per CTA of the pair kernel
 // u32 words per window slot: the three signed sums (didj, di, dj) as 22+22+rest
 // bit words of a 62-bit fixed-point value, the four positive sums (wgt, wi,
@@ -83,6 +84,11 @@ struct PairArgs {
                              // pixel-pair kernel skips those and evaluates the rest exactly
   double run_amin;           // Cartesian: smallest 2(1 - cos theta) the run sweep accepts
   const float* thr;          // run sweep: first-axis thresholds T[0..n0]
+  // boundary table of the catalogue's common first-axis grid (grid sweep)
+  const uint16_t* gq;        // [2][ng][n0 + 1]: first grid index of bin >= k (side 0, 1)
+  const uint32_t* gfirst;    // per sightline: grid index of pixel 0, or kNoGrid
+  int ng;                    // grid values
+  int grid_split;            // the grid kernel takes the run items whose sightlines are on the grid
   int win_w1;                // window width along axis 1 (Cartesian)
   int win_slots;             // slots per warp window
   unsigned long long* acc;   // [n_cells][ntotal][kAccWords] 128-bit fixed point
@@ -95,6 +101,11 @@ struct PairArgs {
 cudaError_t launch_pair_kernel(const PairArgs& a, int coord, bool exact0, bool minpos, int grid,
                                cudaStream_t stream);
 size_t pair_kernel_smem(int win_slots);
+
+// Launch the persistent grid-sweep kernel (xi_grid.cu) over the items that
+// run_item() accepts and whose two sightlines lie on the common grid.
+cudaError_t launch_grid_kernel(const PairArgs& a, int coord, bool minpos, int num_sms,
+                               cudaStream_t stream);
 
 // Launch the persistent run-sweep kernel (xi_runs.cu) over the items that
 // run_item() accepts: Cartesian and observing coordinates, catalogue sorted
