@@ -115,6 +115,7 @@ typedef struct {
   uint64_t num_run_items;            /* sightline pairs counted by the boundary-sweep kernels */
   double ms_runs;                    /* device time: grid- and run-sweep kernels (part of ms_pairs) */
   uint64_t num_grid_items;           /* of num_run_items: sightline pairs counted by the grid-sweep kernel */
+  double ms_grid;                    /* device time: grid-sweep kernel (part of ms_runs) */
 } tos_xi_stats;
 
 /* Opaque handles. */

@@ -224,3 +224,34 @@ def test_full_size_small_config_cell_subset(engine):
     for c in subset:
         assert_counts_equal(cells[c], ocells[c])
         assert_sums_close(cells[c], ocells[c], acells[c])
+
+
+def drop_pixels(los, px, frac, seed):
+    """Remove a random fraction of the pixels of every other sightline (as
+    masking does): those sightlines are no longer contiguous on the grid."""
+    rng = np.random.default_rng(seed)
+    los2 = los.copy()
+    out, off = [], 0
+    for s in range(len(los)):
+        o, n = int(los[s]["pixel_offset"]), int(los[s]["num_pixels"])
+        p = px[o:o + n]
+        if s % 2 == 1 and n > 4:
+            p = p[np.sort(rng.choice(n, size=max(2, int(n * (1 - frac))), replace=False))]
+        out.append(p)
+        los2[s]["pixel_offset"] = off
+        los2[s]["num_pixels"] = len(p)
+        off += len(p)
+    return los2, np.concatenate(out)
+
+
+@pytest.mark.parametrize("name", ["cartesian", "observing", "cartesian_gap"])
+def test_pointer_sweep_on_gapped_sightlines(engine, name):
+    los, px, meta = small_catalog(n=120, seed=21, size_deg=2.5)
+    los, px = drop_pixels(los, px, 0.1, seed=4)
+    g = ALL_GRIDS[name]
+    bins, cells, ids, st, obins, ocells, oids, ost = run_both(engine, los, px, g, meta["scale"])
+    assert_counts_equal(bins, obins)
+    assert_sums_close(bins, obins, ost["abs"])
+    # both sweeps ran: grid pairs and pairs with a gapped sightline
+    assert 0 < st["num_grid_items"] < st["num_run_items"]
+    assert st["num_run_items"] == st["num_sightline_pairs_used"]

@@ -1111,6 +1111,7 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
       if (ge2 != cudaSuccess)
         return fail(TOS_ERR_CUDA, std::string("grid kernel: ") + cudaGetErrorString(ge2));
     }
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[6], st));
     if (use_runs) {
       PairArgs R = A;
       R.next_item = ctr + 7;
@@ -1125,6 +1126,7 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
     TOS_CUDA_TRY(cudaEventRecord(e->ev[3], st));
   } else {
     TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[6], st));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[3], st));
   }
@@ -1173,6 +1175,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
     stats->ms_device = ms;
     cudaEventElapsedTime(&ms, e->ev[2], e->ev[5]);
     stats->ms_runs = ms;
+    cudaEventElapsedTime(&ms, e->ev[2], e->ev[6]);
+    stats->ms_grid = ms;
     stats->num_run_items = hc[8] + hc[9];
     stats->num_grid_items = hc[9];
     stats->ms_total =

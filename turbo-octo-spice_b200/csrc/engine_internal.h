@@ -65,7 +65,7 @@ struct tos_engine {
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[7] = {};
   std::mutex mu;
 };
 

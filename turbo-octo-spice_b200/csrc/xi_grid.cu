@@ -28,7 +28,14 @@ __device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, 
   const bool act = task < 2 * n0;
   const int side = act ? task / n0 : 0;
   const int k = act ? task % n0 : 0;
-  const int nj = it.nj;
+  // the item in registers: the loop's flushes would force reloads from memory
+  const int nj = it.nj, r_lo = it.r_lo, r_hi = it.r_hi;
+  const Dest d = it.d;
+  const double c = it.c;
+  const float ap = it.ap, inv1sqf = A.inv1sqf;
+  const float *rowd = it.rowd, *rowl = it.rowl, *roww = it.roww, *colx = it.colx;
+  const double* rowwd = it.rowwd;
+  const double4* pre = it.pre;
   const size_t qstride = (size_t)(n0 + 1);
   const uint16_t* qrow = A.gq + ((size_t)side * A.ng + fi) * qstride + k;
   RunAcc acc;
@@ -38,23 +45,23 @@ __device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, 
   unsigned rech = 0;
   unsigned long long n_eval = 0;
   // boundaries loaded one row ahead
-  ushort2 nQ = make_ushort2(qrow[(size_t)it.r_lo * qstride], qrow[(size_t)it.r_lo * qstride + 1]);
+  ushort2 nQ = make_ushort2(qrow[(size_t)r_lo * qstride], qrow[(size_t)r_lo * qstride + 1]);
 #pragma unroll 1
-  for (int r = it.r_lo; r < it.r_hi; ++r) {
+  for (int r = r_lo; r < r_hi; ++r) {
     const ushort2 Qv = nQ;
-    const int rn = min(r + 1, it.r_hi - 1);
+    const int rn = min(r + 1, r_hi - 1);
     nQ = make_ushort2(qrow[(size_t)rn * qstride], qrow[(size_t)rn * qstride + 1]);
     const int qa = min(max((int)Qv.x - fj, 0), nj), qb = min(max((int)Qv.y - fj, 0), nj);
     const int s = side ? qb : qa, e = side ? qa : qb;
     if (act && e > s) {
       n_eval += (unsigned long long)(e - s);
-      const RowV R = row_values<COORD>(A, it, r);
-      do_run<COORD, MINPOS>(A, it.d, it.colx, it.pre, it.c, R, k, s, e, acc, rech);
+      const RowV R = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, r);
+      do_run<COORD, MINPOS>(A, d, colx, pre, c, R, k, s, e, acc, rech);
     }
   }
   if (act) {
-    acc_flush8<COORD>(A, it.d, k, acc.B, acc.s0);
-    acc_flush8<COORD>(A, it.d, k, acc.B + 1, acc.s1);
+    acc_flush8<COORD>(A, d, k, acc.B, acc.s0);
+    acc_flush8<COORD>(A, d, k, acc.B + 1, acc.s1);
   }
   stats[0] += n_eval;
   stats[1] += rech;

@@ -48,12 +48,19 @@ __device__ __noinline__ void run_group(const PairArgs& A, const SweepItem& it, i
   const bool act = task < 2 * n0;
   const int side = act ? task / n0 : 0;
   const int k = act ? task % n0 : 0;
-  const int nj = it.nj;
+  // the item in registers: the loop's flushes would force reloads from memory
+  const int nj = it.nj, r_lo = it.r_lo, r_hi = it.r_hi;
+  const Dest d = it.d;
+  const double c = it.c;
+  const float ap = it.ap, inv1sqf = A.inv1sqf;
+  const float *rowd = it.rowd, *rowl = it.rowl, *roww = it.roww, *rowx = it.rowx, *colx = it.colx;
+  const double* rowwd = it.rowwd;
+  const double4* pre = it.pre;
   const float ta = A.thr[k], tb = A.thr[k + 1];
-  const float x1f = it.rowx[it.r_lo];
+  const float x1f = rowx[r_lo];
   ColPtr pa, pb;
-  pa.init(it.colx, bsearch_col(it.colx, 0, nj, [&](float x2) { return ptr_pred(side, x1f, x2, ta); }));
-  pb.init(it.colx, bsearch_col(it.colx, 0, nj, [&](float x2) { return ptr_pred(side, x1f, x2, tb); }));
+  pa.init(colx, bsearch_col(colx, 0, nj, [&](float x2) { return ptr_pred(side, x1f, x2, ta); }));
+  pb.init(colx, bsearch_col(colx, 0, nj, [&](float x2) { return ptr_pred(side, x1f, x2, tb); }));
   RunAcc acc;
   acc.B = -1;
 #pragma unroll
@@ -61,21 +68,21 @@ __device__ __noinline__ void run_group(const PairArgs& A, const SweepItem& it, i
   unsigned rech = 0;
   unsigned long long n_eval = 0;
 #pragma unroll 1
-  for (int r = it.r_lo; r < it.r_hi; ++r) {
-    const float x1 = it.rowx[r];
+  for (int r = r_lo; r < r_hi; ++r) {
+    const float x1 = rowx[r];
     if (!act) continue;
-    pa.advance(it.colx, nj, side, x1, ta);
-    pb.advance(it.colx, nj, side, x1, tb);
+    pa.advance(colx, nj, side, x1, ta);
+    pb.advance(colx, nj, side, x1, tb);
     const int s = side ? pb.p : pa.p, e = side ? pa.p : pb.p;
     if (e > s) {
       n_eval += (unsigned long long)(e - s);
-      const RowV R = row_values<COORD>(A, it, r);
-      do_run<COORD, MINPOS>(A, it.d, it.colx, it.pre, it.c, R, k, s, e, acc, rech);
+      const RowV R = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, r);
+      do_run<COORD, MINPOS>(A, d, colx, pre, c, R, k, s, e, acc, rech);
     }
   }
   if (act) {
-    acc_flush8<COORD>(A, it.d, k, acc.B, acc.s0);
-    acc_flush8<COORD>(A, it.d, k, acc.B + 1, acc.s1);
+    acc_flush8<COORD>(A, d, k, acc.B, acc.s0);
+    acc_flush8<COORD>(A, d, k, acc.B + 1, acc.s1);
   }
   stats[0] += n_eval;
   stats[1] += rech;

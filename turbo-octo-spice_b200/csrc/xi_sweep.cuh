@@ -295,17 +295,18 @@ __device__ __forceinline__ bool load_item(const PairArgs& A, unsigned long long 
 
 // Row r of an item.
 template <int COORD>
-__device__ __forceinline__ RowV row_values(const PairArgs& A, const SweepItem& it, int r) {
+__device__ __forceinline__ RowV row_values(const float* rowd, const double* rowwd, const float* roww,
+                                           const float* rowl, float ap, float inv1sqf, int r) {
   RowV R;
-  R.d1 = it.rowd[r];
-  R.wd1 = it.rowwd[r];
-  R.w1 = (double)it.roww[r];
-  R.hl1 = 0.5 * (double)it.rowl[r];
+  R.d1 = rowd[r];
+  R.wd1 = rowwd[r];
+  R.w1 = (double)roww[r];
+  R.hl1 = 0.5 * (double)rowl[r];
   if (COORD == kCart) {
     const float p = __fmul_rn(R.d1, R.d1);
     const float err = __fmaf_rn(R.d1, R.d1, -p);  // d1*d1 = p + err exactly
-    R.A1 = __fmul_rn(R.d1, it.ap);
-    R.dl1 = __fmul_rn(-err, A.inv1sqf);
+    R.A1 = __fmul_rn(R.d1, ap);
+    R.dl1 = __fmul_rn(-err, inv1sqf);
   } else {
     R.A1 = R.dl1 = 0.f;
   }

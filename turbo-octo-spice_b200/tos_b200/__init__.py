@@ -52,7 +52,7 @@ class XiStats(C.Structure):
         "num_pixel_pairs", "num_pixel_pairs_used", "num_pixel_pairs_evaluated", "num_edge_rechecks",
         "num_index_overflow", "num_cells", "num_direct_runs", "num_window_flushes")] + [(n, C.c_double) for n in (
             "max_ang", "cos_max_ang", "ms_expand", "ms_pairs", "ms_total", "ms_device")] + [
-        ("num_run_items", C.c_uint64), ("ms_runs", C.c_double), ("num_grid_items", C.c_uint64)]
+        ("num_run_items", C.c_uint64), ("ms_runs", C.c_double), ("num_grid_items", C.c_uint64), ("ms_grid", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
