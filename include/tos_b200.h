@@ -198,6 +198,25 @@ tos_status tos_brute_run(tos_engine* engine, const float* points, size_t n_point
                          double max, int nbins, double* dsum, double* wsum, uint64_t* counts,
                          double* ms_kernel);
 
+/* tos_brute_run without any device allocation.  No counterpart in the
+ * reference: it is for callers that cannot allocate GPU memory while they
+ * count pairs (memory managed entirely by their own pool, code where a
+ * cudaMalloc would synchronise the device or is not allowed, loops that must
+ * not touch the allocator).  points (n_points x 5 floats: x, y, z, delta, w),
+ * dsum, wsum and counts (nbins + 2 each) are DEVICE pointers on the engine's
+ * device; results equal tos_brute_run's.  All scratch lives in one static
+ * device array of about 12.7 MB that the library reserves on every GPU that
+ * loads it, until the process exits, which limits a call to n_points <=
+ * 262144 and nbins <= 4096 (larger requests fail with TOS_ERR_INVALID_ARG).
+ * The first call on a device looks up that array (and may load the module
+ * on the device): make it before any stream capture.  Every call shares the
+ * array, so calls that overlap on the GPU (other engines or threads on the
+ * same device) race; the call synchronises the engine's stream before it
+ * returns. */
+tos_status tos_brute_run_noalloc(tos_engine* engine, const float* points, size_t n_points,
+                                 double min, double max, int nbins, double* dsum, double* wsum,
+                                 uint64_t* counts, double* ms_kernel);
+
 /* ---- flat LCDM comoving distance (h5healxi.cc:123-131, 196-203) ---------- */
 
 /* Line-of-sight comoving distance in Mpc/h of a flat universe with the given

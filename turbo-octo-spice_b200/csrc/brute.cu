@@ -337,3 +337,194 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
   }
   return TOS_OK;
 }
+
+// ============================================================================
+// Allocation-free variant of tos_brute_run.
+//
+// Some callers cannot allocate device memory while they count pairs: code
+// that manages every byte of the GPU through its own pool, code that runs
+// where a cudaMalloc would synchronise the device or is not allowed (for
+// instance between the start and end of a stream capture), or service loops
+// that must not touch the allocator at all.  tos_brute_run allocates its
+// scratch on every call; tos_brute_run_noalloc takes its inputs and outputs
+// in device memory and keeps all scratch in one statically sized device
+// array that the library reserves on every GPU that loads it, until exit.
+// ============================================================================
+
+namespace tos {
+namespace {
+
+constexpr size_t kNoAllocMaxPoints = size_t(1) << 18;  // 262,144 points (a 64^3 grid)
+constexpr int kNoAllocMaxBins = 4096;
+
+constexpr size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+// scratch layout (byte offsets, each 256-byte aligned)
+constexpr size_t kNaPos = 0;                                                  // float4[n]
+constexpr size_t kNaWd = kNaPos + round256(16 * kNoAllocMaxPoints);           // double[n]
+constexpr size_t kNaW = kNaWd + round256(8 * kNoAllocMaxPoints);              // double[n]
+constexpr size_t kNaPrefix = kNaW + round256(8 * kNoAllocMaxPoints);          // double2[n + 1]
+constexpr size_t kNaOut = kNaPrefix + round256(16 * (kNoAllocMaxPoints + 1));  // double[2 (nbins + 2)]
+constexpr size_t kNaCounts = kNaOut + round256(16 * (kNoAllocMaxBins + 2));   // u64[nbins + 2]
+constexpr size_t kNaMisc = kNaCounts + round256(8 * (kNoAllocMaxBins + 2));   // u64[8]
+constexpr size_t kNoAllocBytes = kNaMisc + 256;                               // ~12.7 MB
+
+// The scratch.  Host code must not pass this name to a kernel: on the host
+// it stands for a host-side shadow, not for the device memory; the device
+// address comes from cudaGetSymbolAddress (noalloc_scratch below).
+static __device__ __align__(256) unsigned char g_brute_scratch[kNoAllocBytes];
+
+// max |w * delta| and max |w| (as ordered bit patterns of non-negative
+// doubles) and a flag for non-finite coordinates, weights or deltas
+__global__ void k_brute_bounds(const float* pts, int n, unsigned long long* maxbits,
+                               unsigned long long* bad) {
+  double mwd = 0, mw = 0;
+  bool nonfinite = false;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const float* p = pts + 5 * (size_t)k;
+    if (!isfinite(p[0]) || !isfinite(p[1]) || !isfinite(p[2]) || !isfinite(p[3]) || !isfinite(p[4]))
+      nonfinite = true;
+    mwd = fmax(mwd, fabs((double)p[4] * (double)p[3]));
+    mw = fmax(mw, fabs((double)p[4]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mwd = fmax(mwd, __shfl_xor_sync(kFull, mwd, o));
+    mw = fmax(mw, __shfl_xor_sync(kFull, mw, o));
+  }
+  nonfinite = __any_sync(kFull, nonfinite);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&maxbits[0], (unsigned long long)__double_as_longlong(mwd));
+    atomicMax(&maxbits[1], (unsigned long long)__double_as_longlong(mw));
+    if (nonfinite) atomicOr(bad, 1ull);
+  }
+}
+
+// interleaved (dsum, wsum) sums and counts -> the caller's three arrays
+__global__ void k_brute_unpack(const double* out, const unsigned long long* cnt, int nb2, double* dsum,
+                               double* wsum, uint64_t* counts) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb2; b += gridDim.x * blockDim.x) {
+    dsum[b] = out[2 * b];
+    wsum[b] = out[2 * b + 1];
+    counts[b] = cnt[b];
+  }
+}
+
+// Device address of g_brute_scratch on `device` (current): looked up once per
+// device; the lookup may load the module on that device.
+tos_status noalloc_scratch(int device, unsigned char** out) {
+  static std::mutex mu;
+  static std::vector<unsigned char*> addr;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((size_t)device >= addr.size()) addr.resize(device + 1, nullptr);
+  if (!addr[device]) {
+    void* p = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_brute_scratch);
+    if (err != cudaSuccess || !p)
+      return fail(TOS_ERR_CUDA, std::string("cudaGetSymbolAddress of the brute scratch: ") +
+                                    cudaGetErrorString(err));
+    addr[device] = (unsigned char*)p;
+  }
+  *out = addr[device];
+  return TOS_OK;
+}
+
+}  // namespace
+}  // namespace tos
+
+extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points, size_t n_points,
+                                            double min, double max, int nbins, double* d_dsum,
+                                            double* d_wsum, uint64_t* d_counts, double* ms_kernel) {
+  if (!e || !d_points || !d_dsum || !d_wsum || !d_counts) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (n_points < 2) return fail(TOS_ERR_INVALID_ARG, "need at least 2 points");
+  if (n_points > kNoAllocMaxPoints)
+    return fail(TOS_ERR_INVALID_ARG, "tos_brute_run_noalloc takes at most " +
+                                         std::to_string(kNoAllocMaxPoints) + " points (got " +
+                                         std::to_string(n_points) + "); use tos_brute_run");
+  if (nbins <= 0 || nbins > kNoAllocMaxBins)
+    return fail(TOS_ERR_INVALID_ARG, "nbins must be in [1, " + std::to_string(kNoAllocMaxBins) + "]");
+  if (!(max > min) || !std::isfinite(min) || !std::isfinite(max))
+    return fail(TOS_ERR_INVALID_ARG, "need finite min < max");
+  std::lock_guard<std::mutex> lock(e->mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(e->device);
+  struct Restore {
+    int d;
+    ~Restore() { cudaSetDevice(d); }
+  } restore{prev};
+  unsigned char* S = nullptr;
+  TOS_TRY(noalloc_scratch(e->device, &S));
+  const int n = (int)n_points;
+  const int nb2 = nbins + 2;
+  cudaStream_t st = e->stream;
+  float4* pos = (float4*)(S + kNaPos);
+  double* wd = (double*)(S + kNaWd);
+  double* w = (double*)(S + kNaW);
+  double2* prefix = (double2*)(S + kNaPrefix);
+  double* out = (double*)(S + kNaOut);
+  unsigned long long* cnt = (unsigned long long*)(S + kNaCounts);
+  unsigned long long* misc = (unsigned long long*)(S + kNaMisc);  // [0] chunk counter [1] rechecks
+                                                                   // [2,3] bounds [4] non-finite
+  // the scratch keeps the previous call's contents: clear what accumulates
+  TOS_CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)nb2 * 2 * sizeof(double), st));
+  TOS_CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)nb2 * sizeof(unsigned long long), st));
+  TOS_CUDA_TRY(cudaMemsetAsync(misc, 0, 8 * sizeof(unsigned long long), st));
+  k_brute_bounds<<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(d_points, n, misc + 2, misc + 4);
+  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_points, n, pos, wd, w);
+  k_brute_scan<<<1, 1024, 0, st>>>(wd, w, n, prefix);
+  TOS_CUDA_TRY(cudaGetLastError());
+  unsigned long long hb[3] = {0, 0, 0};
+  TOS_CUDA_TRY(cudaMemcpyAsync(hb, misc + 2, sizeof(hb), cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  if (hb[2]) return fail(TOS_ERR_INVALID_ARG, "points must be finite");
+  double mwd, mw;
+  std::memcpy(&mwd, &hb[0], 8);
+  std::memcpy(&mw, &hb[1], 8);
+  mwd = std::max(mwd, 1e-300);
+  mw = std::max(mw, 1e-300);
+  // the same kernel arguments as tos_brute_run, pointing into the scratch
+  BruteArgs A{};
+  A.pos = pos;
+  A.prefix = prefix;
+  A.wd = wd;
+  A.w = w;
+  A.n = n;
+  A.nbins = nbins;
+  A.min = min;
+  A.max = max;
+  A.spacing = (max - min) / nbins;
+  A.invf = (float)(1.0 / A.spacing);
+  A.offf = (float)(-min / A.spacing);
+  A.nbf = (float)nbins;
+  A.nbp1f = (float)nbins + 1.0f;
+  int bl = 0;
+  for (uint32_t v = (uint32_t)nbins + 2; v; v >>= 1) ++bl;
+  A.k = std::max(0, std::min(13, 21 - bl));
+  A.mag = std::ldexp(1.5f, 23 - A.k);
+  std::memcpy(&A.bits, &A.mag, 4);
+  const double per[2] = {mwd * kRunCap * mwd, mw * kRunCap * mw};
+  for (int f = 0; f < 2; ++f) {
+    const int F = (int)std::floor(38.0 - std::log2(per[f]));
+    A.scale[f] = std::ldexp(1.0, F);
+    A.inv_scale[f] = std::ldexp(1.0, -F);
+  }
+  A.out = out;
+  A.counts = cnt;
+  A.next = misc;
+  A.counters = misc + 1;
+  const size_t smem = (size_t)kBruteWarps * kBWords * nb2 * sizeof(uint32_t);
+  TOS_CUDA_TRY(cudaFuncSetAttribute(brute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
+  brute_kernel<<<e->num_sms, kBruteWarps * 32, smem, st>>>(A);
+  TOS_CUDA_TRY(cudaGetLastError());
+  TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
+  k_brute_unpack<<<(nb2 + 255) / 256, 256, 0, st>>>(out, cnt, nb2, d_dsum, d_wsum, d_counts);
+  TOS_CUDA_TRY(cudaGetLastError());
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  if (ms_kernel) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev[4], e->ev[5]);
+    *ms_kernel = ms;
+  }
+  return TOS_OK;
+}

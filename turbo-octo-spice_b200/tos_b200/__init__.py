@@ -87,6 +87,7 @@ def lib() -> C.CDLL:
         L.tos_xibin_finalize.argtypes = [vp, sz]
         L.tos_xibin_finalize.restype = None
         L.tos_brute_run.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
+        L.tos_brute_run_noalloc.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
         L.tos_comoving_distance.argtypes = [dbl, vp, sz, vp]
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
         for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
@@ -274,6 +275,19 @@ def brute_run(engine: Engine, points: np.ndarray, rmin: float, rmax: float, nbin
     _check(lib().tos_brute_run(engine.handle, _ptr(pts), len(pts), rmin, rmax, nbins, _ptr(dsum), _ptr(wsum),
                                _ptr(counts), C.byref(ms)))
     return dsum, wsum, counts, ms.value
+
+
+def brute_run_noalloc(engine: Engine, points_ptr: int, n_points: int, rmin: float, rmax: float,
+                      nbins: int, dsum_ptr: int, wsum_ptr: int, counts_ptr: int) -> float:
+    """tos_brute_run_noalloc: the brute-force count on device buffers with no
+    device allocation (for callers that cannot allocate GPU memory).  The
+    arguments are device addresses: points (n, 5) float32, dsum and wsum
+    float64 (nbins+2), counts uint64 (nbins+2).  Returns the kernel ms."""
+    ms = C.c_double()
+    _check(lib().tos_brute_run_noalloc(engine.handle, C.c_void_p(points_ptr), n_points, rmin, rmax, nbins,
+                                       C.c_void_p(dsum_ptr), C.c_void_p(wsum_ptr), C.c_void_p(counts_ptr),
+                                       C.byref(ms)))
+    return ms.value
 
 
 def comoving_distance(omega_matter: float, z) -> np.ndarray:
