@@ -2,7 +2,9 @@
 
 TEST INFRASTRUCTURE: used by tests/, __graft_entry__.smoke() and the CPU
 baseline leg of bench.py only, as the checker or the timed reference CPU path.
-The engine never loads it.
+The engine never loads it.  Parity unpinned: the reference ships no expected
+outputs for this path and cannot be built here; see the header of
+xi_oracle.c for what the oracle is checked against.
 """
 from __future__ import annotations
 

@@ -29,6 +29,13 @@
  * query_disc_inclusive: both return every sightline within max_ang, and the
  * exact cos cut decides, so the accepted pairs are the same.
  *
+ * Parity unpinned: the reference ships no expected outputs for this path, and
+ * its own code cannot be built here (XiEstimator.cc needs boost, likely,
+ * Healpix_cxx and cosmo).  This restatement is checked against a literal
+ * transcription of the reference's loop (tests/ref_loop.py), hand-built
+ * known answers at bin edges, and HEALPix known pixels; tests/golden holds
+ * fixtures generated from it (tests/golden/make_golden.py).
+ *
  * static_cast<unsigned>(double) is reproduced as the x86-64 code of the
  * reference build computes it (cvttsd2si into 64 bits, low 32 bits kept).
  * Build strictly (-fno-fast-math -ffp-contract=off) for parity.

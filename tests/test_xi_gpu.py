@@ -201,6 +201,10 @@ def test_invalid_inputs(engine):
     cat = T.Catalog(engine, los, px, 6)
     with pytest.raises(T.TosError):
         T.xi_run(engine, cat, T.Grid.cartesian(), -1.0)
+    # bins so fine that a separation's index would wrap 32 bits
+    with pytest.raises(T.TosError) as e:
+        T.xi_run(engine, cat, T.Grid.cartesian("[0:1e-6]*50"), meta["scale"])
+    assert e.value.status == 5  # TOS_ERR_UNSUPPORTED
 
 
 def test_full_size_small_config_cell_subset(engine):

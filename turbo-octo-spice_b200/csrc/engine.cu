@@ -813,6 +813,20 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   cudaStream_t st = e->stream;
   const tos_grid& G = *grid;
   const RefGrid rg = make_ref_grid(G);
+  {
+    // separations are at most twice the largest |coordinate|; a bin index
+    // computed from one must stay below 2^31, where the reference's 32-bit
+    // cast would wrap it back into the grid
+    const double xr = (G.type == TOS_OBSERVING) ? 2.0 * cat->max_l : 2.0 * cat->max_d;
+    const double span0 = (xr * (1.0 + 1e-6) + 1.0 + std::fabs(rg.min0)) * rg.inv0;
+    const double span1 = (G.type == TOS_CARTESIAN)
+                             ? (xr * (1.0 + 1e-6) + 1.0 + std::fabs(rg.min1)) * rg.inv1
+                             : 0.0;
+    if (!(span0 < 2147483648.0) || !(span1 < 2147483648.0))
+      return fail(TOS_ERR_UNSUPPORTED,
+                  "grid bins too fine for the catalogue's coordinates: a separation's bin index "
+                  "would pass 2^31 and wrap the reference's 32-bit index");
+  }
   const uint32_t nb = rg.ntotal;
   const uint32_t nc = (uint32_t)cat->cells.size();
   const double max_ang = max_angular_scale(G, scale);
