@@ -181,6 +181,27 @@ size_t tos_grid_num_bins(const tos_grid* grid);
 tos_status tos_xi_run(tos_engine* engine, tos_catalog* catalog, const tos_grid* grid, double scale,
                       uint32_t flags, tos_xibin* out_bins, tos_xibin* out_cells, tos_xi_stats* stats);
 
+/* Covariance of the per-cell correlation functions of the last tos_xi_run on
+ * `catalog` (XiEstimator::run with do_cov, XiEstimator.cc:60-97).  Every
+ * occupied cell c is a sample x_c[b] = didj/wgt (0 where wgt = 0) of weight
+ * W_c = sum of wgt over its bins with wgt > 0; mean = sum_c W_c x_c / W and
+ * cov = sum_c W_c (x_c - mean)(x_c - mean)^T / W with W = sum_c W_c
+ * (n_bins x n_bins, row-major; n_bins of that run).  The reference hands the
+ * samples to likely::CovarianceAccumulator, whose source is not part of it;
+ * this is the weighted covariance.  mean and total_weight may be NULL. */
+tos_status tos_xi_cell_covariance(tos_engine* engine, tos_catalog* catalog, double* mean, double* cov,
+                                  double* total_weight);
+/* Jackknife of the last tos_xi_run on `catalog` over the HEALPix pixels of
+ * order region_order (<= the catalogue's order) that hold occupied cells:
+ * region k's estimate xi_jk[k][b] = (D - D_k) / (G - G_k), where D and G are
+ * the run's didj and wgt sums of bin b and D_k, G_k those of the cells inside
+ * region k (subtracted exactly; 0 where G - G_k <= 0), and
+ * cov = (N - 1)/N sum_k (xi_k - mean)(xi_k - mean)^T over the N regions.
+ * With region_ids, xi_jk or cov NULL only *n_regions is set (size query);
+ * otherwise cap must be >= N; region_ids ascending, xi_jk [N][n_bins]. */
+tos_status tos_xi_jackknife(tos_engine* engine, tos_catalog* catalog, int region_order, size_t cap,
+                            size_t* n_regions, int64_t* region_ids, double* xi_jk, double* cov);
+
 /* XiBin::finalize (types.h:96-101) applied to n bins in place. */
 void tos_xibin_finalize(tos_xibin* bins, size_t n);
 

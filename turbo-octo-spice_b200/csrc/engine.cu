@@ -811,6 +811,7 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   std::lock_guard<std::mutex> lock(e->mu);
   DeviceGuard dg(e->device);
   cudaStream_t st = e->stream;
+  cat->last_valid = false;
   const tos_grid& G = *grid;
   const RefGrid rg = make_ref_grid(G);
   {
@@ -1162,6 +1163,9 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  cat->last_valid = true;
+  cat->last_nb = nb;
+  for (int k = 0; k < 7; ++k) cat->last_inv_scale[k] = 1.0 / A.scale[k];
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->num_sightlines = cat->n_los;

@@ -123,5 +123,9 @@ struct tos_catalog {
   tos::DevBuf<float> d_grid[2];                        // sorted distinct values
   tos::DevBuf<uint32_t> d_gfirst[2];                   // per sightline grid index of pixel 0 or kNoGrid
   tos::DevBuf<uint16_t> d_gq;                          // boundary table of the current call
+  // the last completed tos_xi_run: its per-cell sums stay in d_acc
+  bool last_valid = false;
+  uint32_t last_nb = 0;
+  double last_inv_scale[7] = {};                       // fixed point -> value, per field
   tos::DevBuf<unsigned char> d_cub_tmp;
 };

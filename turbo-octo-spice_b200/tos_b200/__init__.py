@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
         L.tos_xibin_finalize.restype = None
         L.tos_brute_run.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
         L.tos_brute_run_noalloc.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
+        L.tos_xi_cell_covariance.argtypes = [vp, vp, vp, vp, vp]
+        L.tos_xi_jackknife.argtypes = [vp, vp, i32, sz, C.POINTER(sz), vp, vp, vp]
         L.tos_comoving_distance.argtypes = [dbl, vp, sz, vp]
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
         for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
@@ -288,6 +290,29 @@ def brute_run_noalloc(engine: Engine, points_ptr: int, n_points: int, rmin: floa
                                        C.c_void_p(dsum_ptr), C.c_void_p(wsum_ptr), C.c_void_p(counts_ptr),
                                        C.byref(ms)))
     return ms.value
+
+
+def cell_covariance(engine: Engine, cat: "Catalog", nbins: int):
+    """Covariance of the per-cell xi of the last xi_run on `cat` (the
+    reference's do_cov).  Returns (mean[nbins], cov[nbins, nbins], total weight)."""
+    mean = np.zeros(nbins)
+    cov = np.zeros((nbins, nbins))
+    W = C.c_double()
+    _check(lib().tos_xi_cell_covariance(engine.handle, cat.handle, _ptr(mean), _ptr(cov), C.byref(W)))
+    return mean, cov, W.value
+
+
+def jackknife(engine: Engine, cat: "Catalog", region_order: int, nbins: int):
+    """Leave-one-region-out jackknife of the last xi_run on `cat` over HEALPix
+    regions of region_order.  Returns (region ids, xi_jk[N, nbins], cov)."""
+    n = C.c_size_t()
+    _check(lib().tos_xi_jackknife(engine.handle, cat.handle, region_order, 0, C.byref(n), None, None, None))
+    ids = np.zeros(n.value, dtype=np.int64)
+    xi = np.zeros((n.value, nbins))
+    cov = np.zeros((nbins, nbins))
+    _check(lib().tos_xi_jackknife(engine.handle, cat.handle, region_order, n.value, C.byref(n), _ptr(ids),
+                                  _ptr(xi), _ptr(cov)))
+    return ids, xi, cov
 
 
 def comoving_distance(omega_matter: float, z) -> np.ndarray:

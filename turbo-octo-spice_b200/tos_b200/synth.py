@@ -242,7 +242,7 @@ def grf_grid(n: int = 64, box: float = 256.0, seed: int = 3, index: float = -2.0
     amp = np.zeros_like(k2)
     nz = k2 > 0
     amp[nz] = k2[nz] ** (index / 4.0)  # sqrt(P) with P ~ k^index
-    field = np.fft.irfftn(fk * amp, s=(n, n, n))
+    field = np.fft.irfftn(fk * amp, s=(n, n, n), axes=(0, 1, 2))
     field /= field.std()
     cell = box / n
     c = (np.arange(n) + 0.5) * cell
