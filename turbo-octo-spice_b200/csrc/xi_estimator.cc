@@ -121,8 +121,8 @@ XiEstimator::~XiEstimator() {
 }
 
 void XiEstimator::run(int /*nthreads*/, bool do_cov) {
-  if (do_cov) throw RuntimeError("covariance estimation is not supported by this engine");
   const size_t nb = (size_t)grid_.getNBinsTotal();
+  cov_.clear();
   size_t nc = 0;
   check(tos_catalog_num_cells(catalog_, &nc));
   std::vector<int64_t> ids(nc);
@@ -138,10 +138,17 @@ void XiEstimator::run(int /*nthreads*/, bool do_cov) {
   std::cout << "Xi estimation complete!" << std::endl << std::endl;
   print_stats();
   std::cout << std::endl;
+  if (do_cov) {
+    // each cell's xi = didj/wgt weighted by its total wgt (XiEstimator.cc:60-97)
+    std::cout << "Estimating covariance..." << std::endl;
+    cov_.assign(nb * nb, 0.0);
+    check(tos_xi_cell_covariance(engine_, catalog_, nullptr, cov_.data(), nullptr));
+    std::cout << "Covariance estimation complete!" << std::endl << std::endl;
+  }
 }
 
 void XiEstimator::save_results(const std::string& outfile) const {
-  // XiEstimator::save_results (XiEstimator.cc:307-361); no .cov (not built)
+  // XiEstimator::save_results (XiEstimator.cc:307-361)
   const int nb = (int)xi_.size();
   {
     std::ofstream f(outfile + ".data");
@@ -156,6 +163,13 @@ void XiEstimator::save_results(const std::string& outfile) const {
         << lexical(xi_[k].di) << ' ' << lexical(xi_[k].dj) << ' ' << lexical(xi_[k].wgt) << ' '
         << lexical((long long)xi_[k].num_pairs) << ' ' << lexical(xi_[k].z) << '\n';
     }
+  }
+  if (!cov_.empty()) {
+    // upper triangle, column by column (XiEstimator.cc:334-345)
+    std::ofstream f(outfile + ".cov");
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row <= col; ++row)
+        f << row << ' ' << col << ' ' << lexical(cov_[(size_t)row * nb + col]) << '\n';
   }
   {
     std::ofstream f(outfile + ".iwgt");

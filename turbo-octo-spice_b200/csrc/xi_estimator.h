@@ -64,7 +64,8 @@ class XiEstimator {
   XiEstimator(const XiEstimator&) = delete;
   XiEstimator& operator=(const XiEstimator&) = delete;
   // nthreads is accepted for interface compatibility; the work runs on the GPU.
-  // do_cov is not supported (covariance is not built) and must be false.
+  // do_cov: also estimate the covariance of the per-cell xi (written as .cov
+  // by save_results), as XiEstimator::run does (XiEstimator.cc:60-97).
   void run(int nthreads = 0, bool do_cov = false);
   void save_results(const std::string& outfile) const;
   void save_subsamples(const std::string& outfile_base) const;
@@ -73,6 +74,8 @@ class XiEstimator {
   const std::vector<tos_xibin>& xi() const { return xi_; }
   const std::map<int64_t, std::vector<tos_xibin>>& skybin_xis() const { return skybin_xis_; }
   const tos_xi_stats& stats() const { return stats_; }
+  // covariance of the last run with do_cov (row-major n_bins x n_bins), empty otherwise
+  const std::vector<double>& covariance() const { return cov_; }
 
  private:
   double scale_;
@@ -83,6 +86,7 @@ class XiEstimator {
   std::vector<tos_xibin> xi_;
   std::map<int64_t, std::vector<tos_xibin>> skybin_xis_;
   tos_xi_stats stats_{};
+  std::vector<double> cov_;
 };
 
 }  // namespace tos
