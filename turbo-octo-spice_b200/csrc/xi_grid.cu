@@ -19,15 +19,21 @@ namespace {
 
 constexpr int kGridWarps = 4;  // warps per CTA of the grid-sweep kernel
 
-// Rows [r_lo, r_hi) of an item for the 32 (side, bin) tasks t0 + lane.
+// Rows [r_lo, r_hi) of an item for the (side, bin) tasks t0 .. t0 + m - 1
+// (m = min(32, tasks left)).  A group of m < 32 tasks splits the rows into
+// P = 32 / m phases: lane = task + m * phase takes rows r_lo + phase + P i,
+// so the last, partial group of a grid costs 1/P of a full pass.
 template <int COORD, bool MINPOS>
 __device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, int fi, int fj,
                                         int t0, int lane, unsigned long long* stats) {
   const int n0 = (int)A.g.n0;
-  const int task = t0 + lane;
-  const bool act = task < 2 * n0;
-  const int side = act ? task / n0 : 0;
-  const int k = act ? task % n0 : 0;
+  const int m = min(32, 2 * n0 - t0);
+  const int P = 32 / m;
+  const bool act = lane < m * P;
+  const int task = t0 + (act ? lane % m : 0);
+  const int phase = act ? lane / m : 0;
+  const int side = task / n0;
+  const int k = task % n0;
   // the item in registers: the loop's flushes would force reloads from memory
   const int nj = it.nj, r_lo = it.r_lo, r_hi = it.r_hi;
   const Dest d = it.d;
@@ -45,11 +51,12 @@ __device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, 
   unsigned rech = 0;
   unsigned long long n_eval = 0;
   // boundaries loaded one row ahead
-  ushort2 nQ = make_ushort2(qrow[(size_t)r_lo * qstride], qrow[(size_t)r_lo * qstride + 1]);
+  const int r0 = min(r_lo + phase, r_hi - 1);
+  ushort2 nQ = make_ushort2(qrow[(size_t)r0 * qstride], qrow[(size_t)r0 * qstride + 1]);
 #pragma unroll 1
-  for (int r = r_lo; r < r_hi; ++r) {
+  for (int r = r_lo + phase; r < r_hi; r += P) {
     const ushort2 Qv = nQ;
-    const int rn = min(r + 1, r_hi - 1);
+    const int rn = min(r + P, r_hi - 1);
     nQ = make_ushort2(qrow[(size_t)rn * qstride], qrow[(size_t)rn * qstride + 1]);
     const int qa = min(max((int)Qv.x - fj, 0), nj), qb = min(max((int)Qv.y - fj, 0), nj);
     const int s = side ? qb : qa, e = side ? qa : qb;

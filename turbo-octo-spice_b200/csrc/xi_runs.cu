@@ -39,15 +39,21 @@ struct ColPtr {
   }
 };
 
-// Rows [r_lo, r_hi) of an item for the 32 (side, bin) tasks t0 + lane.
+// Rows [r_lo, r_hi) of an item for the (side, bin) tasks t0 .. t0 + m - 1
+// (m = min(32, tasks left)); a partial group splits the rows into P = 32 / m
+// phases, lane = task + m * phase taking rows r_lo + phase + P i (the
+// pointers still only move right).
 template <int COORD, bool MINPOS>
 __device__ __noinline__ void run_group(const PairArgs& A, const SweepItem& it, int t0, int lane,
                                        unsigned long long* stats) {
   const int n0 = (int)A.g.n0;
-  const int task = t0 + lane;
-  const bool act = task < 2 * n0;
-  const int side = act ? task / n0 : 0;
-  const int k = act ? task % n0 : 0;
+  const int m = min(32, 2 * n0 - t0);
+  const int P = 32 / m;
+  const bool act = lane < m * P;
+  const int task = t0 + (act ? lane % m : 0);
+  const int phase = act ? lane / m : 0;
+  const int side = task / n0;
+  const int k = task % n0;
   // the item in registers: the loop's flushes would force reloads from memory
   const int nj = it.nj, r_lo = it.r_lo, r_hi = it.r_hi;
   const Dest d = it.d;
@@ -57,7 +63,7 @@ __device__ __noinline__ void run_group(const PairArgs& A, const SweepItem& it, i
   const double* rowwd = it.rowwd;
   const double4* pre = it.pre;
   const float ta = A.thr[k], tb = A.thr[k + 1];
-  const float x1f = rowx[r_lo];
+  const float x1f = rowx[min(r_lo + phase, r_hi - 1)];
   ColPtr pa, pb;
   pa.init(colx, bsearch_col(colx, 0, nj, [&](float x2) { return ptr_pred(side, x1f, x2, ta); }));
   pb.init(colx, bsearch_col(colx, 0, nj, [&](float x2) { return ptr_pred(side, x1f, x2, tb); }));
@@ -68,7 +74,7 @@ __device__ __noinline__ void run_group(const PairArgs& A, const SweepItem& it, i
   unsigned rech = 0;
   unsigned long long n_eval = 0;
 #pragma unroll 1
-  for (int r = r_lo; r < r_hi; ++r) {
+  for (int r = r_lo + phase; r < r_hi; r += P) {
     const float x1 = rowx[r];
     if (!act) continue;
     pa.advance(colx, nj, side, x1, ta);
