@@ -60,12 +60,16 @@ typedef struct {
 /* One sightline.  Position in radians (ra in [0, 2pi), dec in [-pi/2, pi/2]),
  * identifiers as in Forest (types.h:56-67), and its pixels as a range of a
  * flat pixel array.  Pixels are expected in increasing loglam order, as
- * HDF5Delta::loadForests produces them (HDF5Delta.cc:62-73). */
+ * HDF5Delta::loadForests produces them (HDF5Delta.cc:62-73).
+ * `group` names the catalogue (mock realisation) the sightline belongs to:
+ * sightlines of different groups never pair, so one resident catalogue can
+ * hold many independent catalogues (0 for a single one, the reference's
+ * case: one XiEstimator per catalogue). */
 typedef struct {
   double ra, dec;
   int32_t forest_id, plate;
   uint64_t pixel_offset;
-  uint32_t num_pixels, reserved;
+  uint32_t num_pixels, group;
 } tos_sightline;
 
 /* A linear axis "[min:max]*nbins" with bin width (max-min)/nbins, the binning
@@ -151,15 +155,21 @@ void tos_catalog_destroy(tos_catalog* catalog);
 /* Number of occupied sky cells (SkyBins::getNBins, SkyBins.h:53). */
 tos_status tos_catalog_num_cells(const tos_catalog* catalog, size_t* n_cells);
 /* Occupied cell ids in ascending order — the key order of
- * XiEstimator::skybin_xis_ (XiEstimator.h:78) and of the subsample files. */
+ * XiEstimator::skybin_xis_ (XiEstimator.h:78) and of the subsample files.
+ * A cell id is group * 2^32 + HEALPix pixel (the pixel alone in group 0). */
 tos_status tos_catalog_cells(const tos_catalog* catalog, int64_t* cell_ids, size_t capacity);
-/* HEALPix cell of each sightline (HealpixBins::ang2pix, HealpixBins.h:58-66). */
+/* Cell id of each sightline (HealpixBins::ang2pix, HealpixBins.h:58-66). */
 tos_status tos_catalog_sightline_cells(const tos_catalog* catalog, int64_t* cells, size_t capacity);
+/* Number of distinct sightline groups, and their ids in ascending order (the
+ * row order of a TOS_XI_PER_GROUP result). */
+tos_status tos_catalog_num_groups(const tos_catalog* catalog, size_t* n_groups);
+tos_status tos_catalog_groups(const tos_catalog* catalog, uint32_t* group_ids, size_t capacity);
 
 /* ---- the hot path: XiEstimator pair counting ----------------------------- */
 
 #define TOS_XI_SUBSAMPLES 0x1u   /* also return per-cell sums (skybin_xis_) */
 #define TOS_XI_EXACT      0x2u   /* evaluate every pixel pair in FP64 (validation path, slow) */
+#define TOS_XI_PER_GROUP  0x4u   /* return per-group sums: one xi per catalogue of a batch */
 
 /* Maximum angular scale of a grid for a transverse comoving scale:
  * CartesianGrid::maxAngularScale (CartesianGrid.h:45-46),
@@ -177,6 +187,14 @@ size_t tos_grid_num_bins(const tos_grid* grid);
  *               ascending cell order as xi_finalize_task does (XiEstimator.cc:298-305).
  *   out_cells : NULL, or n_cells*n_bins raw per-cell sums (cell-major, cells
  *               ascending) when flags has TOS_XI_SUBSAMPLES.
+ * With TOS_XI_PER_GROUP (not combined with TOS_XI_SUBSAMPLES) out_cells
+ * receives n_groups*n_bins sums instead, group-major in ascending group id:
+ * group g's row is its cells merged in ascending order, with the pair counts
+ * of running that group alone and the sums to within the fixed-point
+ * rounding (about 1e-12 relative), and out_bins is the sum of the groups'
+ * rows in ascending group order.  This is the batched form of running
+ * XiEstimator once per mock catalogue: every group's pairs go through one
+ * set of launches.
  *   stats     : optional counters and timings. */
 tos_status tos_xi_run(tos_engine* engine, tos_catalog* catalog, const tos_grid* grid, double scale,
                       uint32_t flags, tos_xibin* out_bins, tos_xibin* out_cells, tos_xi_stats* stats);
@@ -201,6 +219,31 @@ tos_status tos_xi_cell_covariance(tos_engine* engine, tos_catalog* catalog, doub
  * otherwise cap must be >= N; region_ids ascending, xi_jk [N][n_bins]. */
 tos_status tos_xi_jackknife(tos_engine* engine, tos_catalog* catalog, int region_order, size_t cap,
                             size_t* n_regions, int64_t* region_ids, double* xi_jk, double* cov);
+
+/* Exact delete-one-region jackknife in one pass over the pairs: the
+ * jackknife subsamples of a batched run.  Region k is a HEALPix RING pixel of
+ * order region_order (<= the catalogue's order) within one sightline group;
+ * a sightline belongs to the region that holds its cell.  Subsample k is the
+ * catalogue without region k's sightlines.  The reference forms it by running
+ * XiEstimator again on the reduced catalogue; here every pair is added to the
+ * slot of its two regions and out_drop[k] = (total of k's group) - (slots
+ * that name k), subtracted exactly in 128-bit fixed point, so each subsample
+ * has the pair counts of that separate run and its sums to within the
+ * fixed-point rounding (about 1e-12 relative).
+ *   flags      : 0 or TOS_XI_EXACT.
+ *   n_regions  : set to the number of (group, region) subsamples N.  With
+ *                region_ids, out_bins or out_drop NULL nothing else happens
+ *                (size query); otherwise capacity must be >= N.
+ *   region_ids : N ids group * 2^32 + region pixel, ascending.
+ *   out_bins   : n_bins sums of the whole catalogue (groups added in order).
+ *   out_groups : NULL or n_groups*n_bins per-group sums (ascending group id).
+ *   out_drop   : N*n_bins raw sums of the subsamples, region-major.
+ * The per-cell sums of this run are not kept: tos_xi_cell_covariance and
+ * tos_xi_jackknife need a tos_xi_run after it. */
+tos_status tos_xi_run_jackknife(tos_engine* engine, tos_catalog* catalog, const tos_grid* grid,
+                                double scale, uint32_t flags, int region_order, size_t capacity,
+                                size_t* n_regions, int64_t* region_ids, tos_xibin* out_bins,
+                                tos_xibin* out_groups, tos_xibin* out_drop, tos_xi_stats* stats);
 
 /* XiBin::finalize (types.h:96-101) applied to n bins in place. */
 void tos_xibin_finalize(tos_xibin* bins, size_t n);

@@ -76,6 +76,19 @@ def assert_sums_close(gpu, ref, ref_abs=None, rel=REL_TOL):
     return errs
 
 
+def assert_same_count(gpu, ref, ref_abs, tol):
+    """Two engine counts of the same pairs (e.g. batched and alone): pair
+    counts equal, and per bin and field |gpu - ref| <= tol * A with A the
+    bin's sum of absolute values of the terms (FP64 oracle, mode 2); the
+    two runs may convert to different fixed-point scales."""
+    assert_counts_equal(gpu, ref)
+    for f in FIELDS:
+        g, r = np.asarray(gpu[f], dtype=np.float64), np.asarray(ref[f], dtype=np.float64)
+        a = np.abs(np.asarray(ref_abs[f], dtype=np.float64))
+        bad = np.nonzero(np.abs(g - r) > tol * a)[0]
+        assert len(bad) == 0, f"field {f}: {len(bad)} bins differ, first {bad[:5]}: {g[bad[:5]]} vs {r[bad[:5]]}"
+
+
 GRIDS = {
     "cartesian": Grid.cartesian(),
     "polar": Grid.polar(),

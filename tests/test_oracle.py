@@ -103,7 +103,7 @@ def test_healpix_known_pixels_and_cross_check():
     rng = np.random.default_rng(1)
     ra = rng.uniform(0, 2 * math.pi, 20000)
     dec = np.arcsin(rng.uniform(-1, 1, 20000))
-    mine = synth._ang2pix_ring_nside8(0.5 * math.pi - dec, ra)
+    mine = synth.ang2pix_ring(8, 0.5 * math.pi - dec, ra)
     orc = np.array([oracle.radec2pix(3, r, d) for r, d in zip(ra, dec)])
     # the vectorised version has no sin(theta) refinement near the poles
     far = np.abs(np.cos(0.5 * math.pi - dec)) < 0.99

@@ -19,25 +19,13 @@
 
 #include "engine_internal.h"
 #include "healpix.h"
+#include "fixed128.cuh"
 #include "xi_kernels.cuh"
 
 namespace tos {
 namespace {
 
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
-
-__device__ __forceinline__ __int128 acc128(const unsigned long long* base, int f) {
-  return (__int128)(((unsigned __int128)(unsigned long long)base[7 + f] << 64) | base[f]);
-}
-
-// Signed 128-bit value as a double with one relative rounding (by magnitude).
-__device__ __forceinline__ double i128_double(__int128 v) {
-  const bool neg = v < 0;
-  const unsigned __int128 m = neg ? (unsigned __int128)(-v) : (unsigned __int128)v;
-  const double d = __fma_rn((double)(unsigned long long)(m >> 64), 18446744073709551616.0 /* 2^64 */,
-                            (double)(unsigned long long)m);
-  return neg ? -d : d;
-}
 
 // One block per cell: x[c][b] = didj/wgt (wgt > 0) else 0, w[c] = sum of wgt > 0.
 __global__ void k_cell_samples(const unsigned long long* acc, uint32_t nb, double inv_didj,
@@ -244,6 +232,8 @@ extern "C" tos_status tos_xi_jackknife(tos_engine* e, tos_catalog* cat, int regi
   if (!n_regions) return fail(TOS_ERR_INVALID_ARG, "n_regions is null");
   if (region_order < 0 || region_order > cat->order)
     return fail(TOS_ERR_INVALID_ARG, "region order must be in [0, catalogue order]");
+  if (cat->groups.size() != 1)
+    return fail(TOS_ERR_INVALID_ARG, "jackknife regions need a catalogue of one sightline group");
   // regions of the occupied cells (a cell lies inside the coarser pixel that
   // holds its centre: both orders tile the same HEALPix hierarchy)
   const int64_t nside_r = (int64_t)1 << region_order;
@@ -251,7 +241,7 @@ extern "C" tos_status tos_xi_jackknife(tos_engine* e, tos_catalog* cat, int regi
   std::vector<int64_t> reg(nc);
   for (size_t c = 0; c < nc; ++c) {
     double th, ph;
-    healpix_pix2ang_ring(cat->nside, cat->cells[c], &th, &ph);
+    healpix_pix2ang_ring(cat->nside, cat->cells[c] & 0xFFFFFFFFll, &th, &ph);
     reg[c] = healpix_ang2pix_ring(nside_r, th, ph);
   }
   std::vector<int64_t> ids(reg);

@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -141,15 +142,18 @@ __global__ void k_prep(const tos_pixel* raw, const uint64_t* off, const uint32_t
 
 // Conservative cell neighbours: cells A, B can hold a sightline pair within
 // max_ang only if the angle between their caps' centres is at most
-// max_ang + r_A + r_B (caps bound every member).
-__global__ void k_cell_neighbours(const double4* cap, uint32_t n_cells, double max_ang,
-                                  const uint32_t* start, uint32_t* count, uint32_t* out) {
+// max_ang + r_A + r_B (caps bound every member).  Only cells of A's own
+// sightline group are searched.
+__global__ void k_cell_neighbours(const double4* cap, const uint2* grange, uint32_t n_cells,
+                                  double max_ang, const uint32_t* start, uint32_t* count,
+                                  uint32_t* out) {
   for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < n_cells;
        a += gridDim.x * blockDim.x) {
     const double4 ca = cap[a];
+    const uint2 gr = grange[a];
     uint32_t n = 0;
     uint32_t o = out ? start[a] : 0;
-    for (uint32_t b = 0; b < n_cells; ++b) {
+    for (uint32_t b = gr.x; b < gr.y; ++b) {
       const double4 cb = cap[b];
       const double lim = max_ang + ca.w + cb.w + 1e-9;
       bool near;
@@ -302,6 +306,68 @@ __global__ void k_combine(const unsigned long long* acc, uint32_t n_cells, uint3
     out[b] = x;
   }
 }
+
+// Per (group, bin): the group's cells merged in ascending cell order, the
+// merge k_combine makes over all cells of a one-group catalogue.
+__global__ void k_combine_groups(const unsigned long long* acc, const uint32_t* gstart,
+                                 uint32_t n_groups, uint32_t nb, double4 inv_a, double4 inv_b,
+                                 tos_xibin* groups_out) {
+  const size_t n = (size_t)n_groups * nb;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t g = (uint32_t)(t / nb), b = (uint32_t)(t % nb);
+    const double inv[7] = {inv_a.x, inv_a.y, inv_a.z, inv_a.w, inv_b.x, inv_b.y, inv_b.z};
+    double s[7] = {0, 0, 0, 0, 0, 0, 0};
+    long long cnt_sum = 0;
+    for (uint32_t c = gstart[g]; c < gstart[g + 1]; ++c) {
+      const unsigned long long* a = acc + ((size_t)c * nb + b) * kAccWords;
+      const long long cnt = (long long)a[14];
+      if (cnt == 0) continue;  // no pairs: zero sums (as k_combine)
+#pragma unroll
+      for (int k = 0; k < 7; ++k) s[k] += i128_to_double(a[k], (long long)a[7 + k]) * inv[k];
+      cnt_sum += cnt;
+    }
+    tos_xibin x;
+    x.didj = s[0];
+    x.di = s[1];
+    x.dj = s[2];
+    x.wgt = s[3];
+    x.wi = s[4];
+    x.wj = s[5];
+    x.z = s[6];
+    x.num_pairs = cnt_sum;
+    groups_out[t] = x;
+  }
+}
+
+// Per bin: the groups' rows added in ascending group order.
+__global__ void k_sum_groups(const tos_xibin* groups, uint32_t n_groups, uint32_t nb,
+                             tos_xibin* out) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    tos_xibin x{};
+    for (uint32_t g = 0; g < n_groups; ++g) {
+      const tos_xibin y = groups[(size_t)g * nb + b];
+      x.didj += y.didj;
+      x.di += y.di;
+      x.dj += y.dj;
+      x.wgt += y.wgt;
+      x.wi += y.wi;
+      x.wj += y.wj;
+      x.z += y.z;
+      x.num_pairs += y.num_pairs;
+    }
+    out[b] = x;
+  }
+}
+
+}  // namespace
+
+void launch_sum_rows(const tos_xibin* rows, uint32_t n_rows, uint32_t nb, tos_xibin* out,
+                     int blocks, cudaStream_t st) {
+  k_sum_groups<<<blocks, 128, 0, st>>>(rows, n_rows, nb, out);
+}
+
+namespace {
 
 int grid_for(const tos_engine* e, size_t work, int block) {
   size_t g = (work + block - 1) / block;
@@ -613,12 +679,29 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
     // SkyObject's cached sines and cosines (types.h:20-26)
     trig[s] = make_double4(std::sin(los[s].dec), std::cos(los[s].dec), std::sin(los[s].ra),
                            std::cos(los[s].ra));
-    cat->cell_of[s] = healpix_radec2pix(cat->nside, los[s].ra, los[s].dec);
+    // cells of different groups never meet: the group is the key's high word
+    cat->cell_of[s] = ((int64_t)los[s].group << 32) |
+                      healpix_radec2pix(cat->nside, los[s].ra, los[s].dec);
   }
   cat->cells = cat->cell_of;
   std::sort(cat->cells.begin(), cat->cells.end());
   cat->cells.erase(std::unique(cat->cells.begin(), cat->cells.end()), cat->cells.end());
   const size_t nc = cat->cells.size();
+  // groups: contiguous ranges of the sorted cells
+  cat->groups.clear();
+  cat->group_cell_start.clear();
+  for (size_t c = 0; c < nc; ++c) {
+    const uint32_t gid = (uint32_t)((uint64_t)cat->cells[c] >> 32);
+    if (cat->groups.empty() || cat->groups.back() != gid) {
+      cat->groups.push_back(gid);
+      cat->group_cell_start.push_back((uint32_t)c);
+    }
+  }
+  cat->group_cell_start.push_back((uint32_t)nc);
+  std::vector<uint2> grange(nc);
+  for (size_t g = 0; g + 1 < cat->group_cell_start.size(); ++g)
+    for (uint32_t c = cat->group_cell_start[g]; c < cat->group_cell_start[g + 1]; ++c)
+      grange[c] = make_uint2(cat->group_cell_start[g], cat->group_cell_start[g + 1]);
   cat->cell_idx.resize(n_los);
   std::vector<uint32_t> ccount(nc + 1, 0);
   for (size_t s = 0; s < n_los; ++s) {
@@ -659,9 +742,12 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
     }
     caps[c] = make_double4(x, y, z, rad * (1 + 1e-9) + 1e-12);
   }
+  cat->caps = caps;
   // --- device buffers
   TOS_TRY(cat->d_trig.alloc(n_los));
   TOS_TRY(cat->d_cap.alloc(nc));
+  TOS_TRY(cat->d_cell_grange.alloc(nc));
+  TOS_TRY(cat->d_group_cell_start.alloc(cat->group_cell_start.size()));
   TOS_TRY(cat->d_cell_idx.alloc(n_los));
   TOS_TRY(cat->d_cell_start.alloc(nc + 1));
   TOS_TRY(cat->d_members.alloc(n_los));
@@ -682,6 +768,10 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
                                cudaMemcpyHostToDevice, st));
   TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cap.p, caps.data(), nc * sizeof(double4),
                                cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cell_grange.p, grange.data(), nc * sizeof(uint2),
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_group_cell_start.p, cat->group_cell_start.data(),
+                               cat->group_cell_start.size() * 4, cudaMemcpyHostToDevice, st));
   TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cell_idx.p, cat->cell_idx.data(), n_los * 4,
                                cudaMemcpyHostToDevice, st));
   TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cell_start.p, cat->cell_start.data(), (nc + 1) * 4,
@@ -766,6 +856,19 @@ tos_status tos_catalog_cells(const tos_catalog* c, int64_t* ids, size_t cap) {
   return TOS_OK;
 }
 
+tos_status tos_catalog_num_groups(const tos_catalog* c, size_t* n) {
+  if (!c || !n) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  *n = c->groups.size();
+  return TOS_OK;
+}
+
+tos_status tos_catalog_groups(const tos_catalog* c, uint32_t* ids, size_t cap) {
+  if (!c || !ids) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (cap < c->groups.size()) return fail(TOS_ERR_INVALID_ARG, "capacity too small");
+  std::copy(c->groups.begin(), c->groups.end(), ids);
+  return TOS_OK;
+}
+
 tos_status tos_catalog_sightline_cells(const tos_catalog* c, int64_t* cells, size_t cap) {
   if (!c || !cells) return fail(TOS_ERR_INVALID_ARG, "null argument");
   if (cap < c->cell_of.size()) return fail(TOS_ERR_INVALID_ARG, "capacity too small");
@@ -797,15 +900,23 @@ void tos_xibin_finalize(tos_xibin* b, size_t n) {
   }
 }
 
-tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, double scale,
-                      uint32_t flags, tos_xibin* out_bins, tos_xibin* out_cells,
-                      tos_xi_stats* stats) {
+}  // extern "C"
+
+namespace tos {
+
+tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, double scale,
+                       uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
+                       tos_xibin* out_cells, tos_xi_stats* stats) {
   const auto t_start = std::chrono::steady_clock::now();
   if (!e || !cat || !out_bins) return fail(TOS_ERR_INVALID_ARG, "null argument");
   if (cat->eng != e) return fail(TOS_ERR_INVALID_ARG, "catalogue belongs to another engine");
   TOS_TRY(check_grid(grid));
   if ((flags & TOS_XI_SUBSAMPLES) && !out_cells)
     return fail(TOS_ERR_INVALID_ARG, "TOS_XI_SUBSAMPLES needs out_cells");
+  if ((flags & TOS_XI_PER_GROUP) && !out_cells)
+    return fail(TOS_ERR_INVALID_ARG, "TOS_XI_PER_GROUP needs out_cells");
+  if ((flags & TOS_XI_PER_GROUP) && (flags & TOS_XI_SUBSAMPLES))
+    return fail(TOS_ERR_INVALID_ARG, "TOS_XI_PER_GROUP and TOS_XI_SUBSAMPLES are exclusive");
   if (grid->type != TOS_OBSERVING && !(scale > 0 && std::isfinite(scale)))
     return fail(TOS_ERR_INVALID_ARG, "scale must be a positive finite number");
   std::lock_guard<std::mutex> lock(e->mu);
@@ -839,8 +950,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   TOS_CUDA_TRY(cudaEventRecord(e->ev[0], st));
   {
     const int gb = grid_for(e, nc, 128);
-    k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, nc, max_ang, nullptr, cat->d_nb_count.p,
-                                          nullptr);
+    k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, cat->d_cell_grange.p, nc, max_ang,
+                                          nullptr, cat->d_nb_count.p, nullptr);
     TOS_CUDA_TRY(cudaGetLastError());
     std::vector<uint32_t> nbc(nc), nbs(nc + 1, 0);
     TOS_CUDA_TRY(cudaMemcpyAsync(nbc.data(), cat->d_nb_count.p, nc * 4, cudaMemcpyDeviceToHost, st));
@@ -849,8 +960,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
     TOS_TRY(cat->d_nb.alloc(nbs[nc]));
     TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_nb_start.p, nbs.data(), (nc + 1) * 4,
                                  cudaMemcpyHostToDevice, st));
-    k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, nc, max_ang, cat->d_nb_start.p, nullptr,
-                                          cat->d_nb.p);
+    k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, cat->d_cell_grange.p, nc, max_ang,
+                                          cat->d_nb_start.p, nullptr, cat->d_nb.p);
     TOS_CUDA_TRY(cudaGetLastError());
   }
   // --- expansion pass 1: counts
@@ -937,7 +1048,8 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   TOS_CUDA_TRY(cudaEventRecord(e->ev[1], st));
 
   // --- accumulation layout and fixed-point scales
-  const size_t acc_words = (size_t)nc * nb * kAccWords;
+  const size_t n_acc_rows = plan ? (size_t)plan->n_rows : (size_t)nc;
+  const size_t acc_words = n_acc_rows * nb * kAccWords;
   TOS_TRY(cat->d_acc.alloc(acc_words));
   TOS_CUDA_TRY(cudaMemsetAsync(cat->d_acc.p, 0, acc_words * 8, st));
   PairArgs A{};
@@ -950,6 +1062,12 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   A.prefix = cat->d_prefix.p;
   A.range = cat->d_range.p;
   A.cell_idx = cat->d_cell_idx.p;
+  if (plan) {
+    A.row_key = plan->row_key;
+    A.slot_start = plan->slot_start;
+    A.slot_key = plan->slot_key;
+    A.spill_row = plan->n_rows - 1;
+  }
   A.item_i = cat->d_item_i.p;
   A.item_j = cat->d_item_j.p;
   A.item_c = cat->d_item_c.p;
@@ -1147,23 +1265,37 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
   }
   // --- combine cells
   const bool want_cells = (flags & TOS_XI_SUBSAMPLES) != 0;
-  TOS_TRY(cat->d_out.alloc((size_t)nb * (want_cells ? (size_t)nc + 1 : 1)));
+  const bool per_group = (flags & TOS_XI_PER_GROUP) != 0;
+  const uint32_t ngr = (uint32_t)cat->groups.size();
+  const size_t n_rows = want_cells ? (size_t)nc : per_group ? (size_t)ngr : 0;
+  TOS_TRY(cat->d_out.alloc((size_t)nb * (n_rows + 1)));
   double4 ia, ib;
   ia.x = 1.0 / A.scale[0], ia.y = 1.0 / A.scale[1], ia.z = 1.0 / A.scale[2], ia.w = 1.0 / A.scale[3];
   ib.x = 1.0 / A.scale[4], ib.y = 1.0 / A.scale[5], ib.z = 1.0 / A.scale[6], ib.w = 0;
-  k_combine<<<grid_for(e, nb, 128), 128, 0, st>>>(cat->d_acc.p, nc, nb, ia, ib, cat->d_out.p,
-                                                   want_cells ? cat->d_out.p + nb : nullptr);
+  if (plan) {
+    double inv[7];
+    for (int k = 0; k < 7; ++k) inv[k] = 1.0 / A.scale[k];
+    TOS_TRY(plan->combine(st, nb, inv, cat->d_out.p));
+  } else if (per_group) {
+    k_combine_groups<<<grid_for(e, (size_t)ngr * nb, 128), 128, 0, st>>>(
+        cat->d_acc.p, cat->d_group_cell_start.p, ngr, nb, ia, ib, cat->d_out.p + nb);
+    TOS_CUDA_TRY(cudaGetLastError());
+    launch_sum_rows(cat->d_out.p + nb, ngr, nb, cat->d_out.p, grid_for(e, nb, 128), st);
+  } else {
+    k_combine<<<grid_for(e, nb, 128), 128, 0, st>>>(cat->d_acc.p, nc, nb, ia, ib, cat->d_out.p,
+                                                     want_cells ? cat->d_out.p + nb : nullptr);
+  }
   TOS_CUDA_TRY(cudaGetLastError());
   TOS_CUDA_TRY(cudaMemcpyAsync(out_bins, cat->d_out.p, (size_t)nb * sizeof(tos_xibin),
                                cudaMemcpyDeviceToHost, st));
-  if (want_cells)
-    TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, cat->d_out.p + nb, (size_t)nc * nb * sizeof(tos_xibin),
+  if (n_rows)
+    TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, cat->d_out.p + nb, n_rows * nb * sizeof(tos_xibin),
                                  cudaMemcpyDeviceToHost, st));
   unsigned long long hc[10];
   TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
-  cat->last_valid = true;
+  cat->last_valid = (plan == nullptr);  // slot rows are not per-cell sums
   cat->last_nb = nb;
   for (int k = 0; k < 7; ++k) cat->last_inv_scale[k] = 1.0 / A.scale[k];
   if (stats) {
@@ -1201,6 +1333,16 @@ tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, dou
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   }
   return TOS_OK;
+}
+
+}  // namespace tos
+
+extern "C" {
+
+tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, double scale,
+                      uint32_t flags, tos_xibin* out_bins, tos_xibin* out_cells,
+                      tos_xi_stats* stats) {
+  return xi_run_impl(e, cat, grid, scale, flags, nullptr, out_bins, out_cells, stats);
 }
 
 }  // extern "C"

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -76,8 +77,11 @@ struct tos_catalog {
   int order = 0;
   int64_t nside = 0;
   // host-side index
-  std::vector<int64_t> cell_of;     // HEALPix pixel of each sightline
+  std::vector<int64_t> cell_of;     // cell id of each sightline: group << 32 | HEALPix pixel
   std::vector<int64_t> cells;       // occupied cells, ascending
+  std::vector<double4> caps;        // per cell: unit centre xyz and angular radius of its members
+  std::vector<uint32_t> groups;     // distinct sightline groups, ascending
+  std::vector<uint32_t> group_cell_start;  // CSR (n_groups+1) into cells
   std::vector<uint32_t> cell_idx;   // per sightline: index into `cells`
   std::vector<uint32_t> cell_start; // CSR (n_cells+1) into members
   std::vector<uint32_t> members;    // sightlines grouped by cell, ascending index within a cell
@@ -86,6 +90,8 @@ struct tos_catalog {
   // device data
   tos::DevBuf<double4> d_trig;      // sin_dec, cos_dec, sin_ra, cos_ra
   tos::DevBuf<double4> d_cap;       // cell cap: unit centre xyz, angular radius
+  tos::DevBuf<uint2> d_cell_grange; // per cell: [first, end) cells of its group
+  tos::DevBuf<uint32_t> d_group_cell_start;  // group_cell_start on the device
   tos::DevBuf<uint32_t> d_cell_idx, d_cell_start, d_members, d_npix;
   tos::DevBuf<uint64_t> d_off;      // compact offset (per-pixel double/float arrays)
   tos::DevBuf<tos_pixel> d_raw;     // uploaded pixels, compact order
@@ -129,3 +135,35 @@ struct tos_catalog {
   double last_inv_scale[7] = {};                       // fixed point -> value, per field
   tos::DevBuf<unsigned char> d_cub_tmp;
 };
+
+namespace tos {
+
+// Accumulation rows of a run other than one per cell: the slots of unordered
+// pairs of sightline keys (rows 0..n_rows-2; row n_rows-1 catches a pair
+// without a slot), and the combine that turns them into the run's results.
+struct RowPlan {
+  uint32_t n_rows = 0;
+  const uint32_t* row_key = nullptr;
+  const uint32_t* slot_start = nullptr;
+  const uint32_t* slot_key = nullptr;
+  // enqueues the combine on the stream: writes the nb run totals to
+  // d_out[0..nb) and any further outputs; inv_scale converts fixed point
+  std::function<tos_status(cudaStream_t, uint32_t nb, const double* inv_scale, tos_xibin* d_out)>
+      combine;
+};
+
+// The pair count behind tos_xi_run: plan = null accumulates per cell (and
+// honours TOS_XI_SUBSAMPLES / TOS_XI_PER_GROUP), otherwise into the plan's
+// slots, combined by plan->combine.  Takes the engine lock.
+tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, double scale,
+                       uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
+                       tos_xibin* out_cells, tos_xi_stats* stats);
+
+// out[b] = rows[0][b] + rows[1][b] + ... (n_rows x nb XiBins, ascending row order).
+void launch_sum_rows(const tos_xibin* rows, uint32_t n_rows, uint32_t nb, tos_xibin* out,
+                     int blocks, cudaStream_t st);
+
+// Maximum angular scale of a grid (the grid classes' maxAngularScale).
+double max_angular_scale(const tos_grid& g, double scale);
+
+}  // namespace tos

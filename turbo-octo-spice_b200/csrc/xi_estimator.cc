@@ -101,7 +101,7 @@ XiEstimator::XiEstimator(double scale, const TwoPointGrid& grid, BinningCoordina
     los[s].plate = f.plate;
     los[s].pixel_offset = px.size();
     los[s].num_pixels = (uint32_t)f.pixels.size();
-    los[s].reserved = 0;
+    los[s].group = 0;
     for (const auto& p : f.pixels) px.push_back({p.value, p.loglam, p.weight, p.distance});
   }
   num_sightlines_ = sightlines.size();

@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) pair_kernel(PairArgs A) {
     it.ni = A.npix[it.i];
     it.nj = A.npix[it.j];
     if (it.ni == 0 || it.nj == 0) continue;
-    it.cell = A.cell_idx[it.i];
+    it.cell = dest_row(A, it.i, it.j);
     it.sep = (COORD == kObs) ? A.item_sep[idx] : 0u;
     const uint64_t oj = A.off[it.j] + (uint64_t)kPad * (it.j + 1);
     it.cold = A.dist_pad + oj;

@@ -58,6 +58,12 @@ struct PairArgs {
   const double4* prefix;     // per sightline, N+1 exclusive prefix sums of (wd, w, loglam)
   const float4* range;       // per sightline (dmin, dmax, lmin, lmax)
   const uint32_t* cell_idx;  // cell index of each sightline
+  // accumulation row of a pair: the primary sightline's cell, or, when
+  // row_key is set, the slot of the unordered pair of the two sightlines' keys
+  const uint32_t* row_key;   // per sightline key, or null
+  const uint32_t* slot_start;// per key a: slots [slot_start[a], slot_start[a+1]) of pairs (a, b >= a)
+  const uint32_t* slot_key;  // per slot: its partner key b
+  uint32_t spill_row;        // row of a pair whose keys have no slot (checked empty by the host)
   // work items
   const uint32_t* item_i;
   const uint32_t* item_j;
@@ -91,11 +97,26 @@ struct PairArgs {
   int grid_split;            // the grid kernel takes the run items whose sightlines are on the grid
   int win_w1;                // window width along axis 1 (Cartesian)
   int win_slots;             // slots per warp window
-  unsigned long long* acc;   // [n_cells][ntotal][kAccWords] 128-bit fixed point
+  unsigned long long* acc;   // [n_rows][ntotal][kAccWords] 128-bit fixed point
   unsigned long long* counters;  // [0] evaluated pairs [1] rechecks [2] overflow pairs
                                  // [3] direct runs [6] window flushes
   int force_exact;           // evaluate every pixel pair with the FP64 reference
 };
+
+// Accumulation row of sightline pair (i, j).
+__device__ __forceinline__ uint32_t dest_row(const PairArgs& A, uint32_t i, uint32_t j) {
+  if (A.row_key == nullptr) return A.cell_idx[i];
+  uint32_t a = A.row_key[i], b = A.row_key[j];
+  if (a > b) {
+    const uint32_t t = a;
+    a = b;
+    b = t;
+  }
+  const uint32_t e = A.slot_start[a + 1];
+  for (uint32_t q = A.slot_start[a]; q < e; ++q)
+    if (A.slot_key[q] == b) return q;
+  return A.spill_row;
+}
 
 // Launch the persistent pixel-pair kernel (coordinate type from a.g/a.* fields).
 cudaError_t launch_pair_kernel(const PairArgs& a, int coord, bool exact0, bool minpos, int grid,

@@ -274,7 +274,7 @@ __device__ __forceinline__ bool load_item(const PairArgs& A, unsigned long long 
   const bool zconst = zlo > -1.0 && zhi < 2147483648.0 && it.d.zb == zbin_of_sum(lsum_hi, A.g);
   it.c = A.item_c[idx];
   if (!run_item(A, it.c, zconst)) return false;
-  it.d.cell = A.cell_idx[it.i];
+  it.d.cell = dest_row(A, it.i, it.j);
   it.d.sep = (COORD == kObs) ? A.item_sep[idx] : 0u;
   const uint64_t oi = A.off[it.i] + (uint64_t)kPad * (it.i + 1);
   const uint64_t oj = A.off[it.j] + (uint64_t)kPad * (it.j + 1);

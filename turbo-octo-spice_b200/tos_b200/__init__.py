@@ -23,11 +23,12 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA", 4: "TIMEOUT", 5:
 POLAR, CARTESIAN, OBSERVING = 0, 1, 2
 XI_SUBSAMPLES = 0x1
 XI_EXACT = 0x2
+XI_PER_GROUP = 0x4
 
 # numpy views of the C structs
 PIXEL_DTYPE = np.dtype([("value", "<f4"), ("loglam", "<f4"), ("weight", "<f4"), ("distance", "<f4")])
 SIGHTLINE_DTYPE = np.dtype([("ra", "<f8"), ("dec", "<f8"), ("forest_id", "<i4"), ("plate", "<i4"),
-                            ("pixel_offset", "<u8"), ("num_pixels", "<u4"), ("reserved", "<u4")])
+                            ("pixel_offset", "<u8"), ("num_pixels", "<u4"), ("group", "<u4")])
 XIBIN_DTYPE = np.dtype([("didj", "<f8"), ("di", "<f8"), ("dj", "<f8"), ("wgt", "<f8"), ("wi", "<f8"),
                         ("wj", "<f8"), ("z", "<f8"), ("num_pairs", "<i8")])
 
@@ -80,6 +81,8 @@ def lib() -> C.CDLL:
         L.tos_catalog_num_cells.argtypes = [vp, C.POINTER(sz)]
         L.tos_catalog_cells.argtypes = [vp, vp, sz]
         L.tos_catalog_sightline_cells.argtypes = [vp, vp, sz]
+        L.tos_catalog_num_groups.argtypes = [vp, C.POINTER(sz)]
+        L.tos_catalog_groups.argtypes = [vp, vp, sz]
         L.tos_grid_max_angular_scale.argtypes = [C.POINTER(_Grid), dbl, C.POINTER(dbl)]
         L.tos_grid_num_bins.argtypes = [C.POINTER(_Grid)]
         L.tos_grid_num_bins.restype = sz
@@ -90,6 +93,8 @@ def lib() -> C.CDLL:
         L.tos_brute_run_noalloc.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
         L.tos_xi_cell_covariance.argtypes = [vp, vp, vp, vp, vp]
         L.tos_xi_jackknife.argtypes = [vp, vp, i32, sz, C.POINTER(sz), vp, vp, vp]
+        L.tos_xi_run_jackknife.argtypes = [vp, vp, C.POINTER(_Grid), dbl, u32, i32, sz, C.POINTER(sz),
+                                           vp, vp, vp, vp, C.POINTER(XiStats)]
         L.tos_comoving_distance.argtypes = [dbl, vp, sz, vp]
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
         for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
@@ -231,6 +236,17 @@ class Catalog:
         _check(lib().tos_catalog_sightline_cells(self._h, _ptr(out), self.n_sightlines))
         return out
 
+    def num_groups(self) -> int:
+        n = C.c_size_t()
+        _check(lib().tos_catalog_num_groups(self._h, C.byref(n)))
+        return n.value
+
+    def groups(self) -> np.ndarray:
+        n = self.num_groups()
+        out = np.zeros(n, dtype=np.uint32)
+        _check(lib().tos_catalog_groups(self._h, _ptr(out), n))
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
             lib().tos_catalog_destroy(self._h)
@@ -244,17 +260,48 @@ class Catalog:
 
 
 def xi_run(engine: Engine, catalog: Catalog, grid: Grid, scale: float, subsamples: bool = False,
-           exact: bool = False):
-    """Pair count of XiEstimator::run. Returns (bins, cells or None, stats dict);
-    bins/cells are raw (unfinalized) XiBin sums as XIBIN_DTYPE arrays."""
+           exact: bool = False, per_group: bool = False):
+    """Pair count of XiEstimator::run. Returns (bins, rows or None, stats dict);
+    bins/rows are raw (unfinalized) XiBin sums as XIBIN_DTYPE arrays.  rows
+    are per cell with subsamples=True, per sightline group (ascending group
+    id, one xi per batched catalogue) with per_group=True."""
     nb = grid.nbins
     bins = np.zeros(nb, dtype=XIBIN_DTYPE)
-    cells = np.zeros((catalog.num_cells(), nb), dtype=XIBIN_DTYPE) if subsamples else None
-    flags = (XI_SUBSAMPLES if subsamples else 0) | (XI_EXACT if exact else 0)
+    cells = None
+    if subsamples:
+        cells = np.zeros((catalog.num_cells(), nb), dtype=XIBIN_DTYPE)
+    elif per_group:
+        cells = np.zeros((catalog.num_groups(), nb), dtype=XIBIN_DTYPE)
+    flags = ((XI_SUBSAMPLES if subsamples else 0) | (XI_EXACT if exact else 0) |
+             (XI_PER_GROUP if per_group else 0))
     st = XiStats()
     _check(lib().tos_xi_run(engine.handle, catalog.handle, C.byref(grid.c_struct()), scale, flags, _ptr(bins),
                             _ptr(cells) if cells is not None else None, C.byref(st)))
     return bins, cells, st.as_dict()
+
+
+def xi_run_jackknife(engine: Engine, catalog: Catalog, grid: Grid, scale: float, region_order: int,
+                     exact: bool = False):
+    """Exact delete-one-region jackknife in one pass (tos_xi_run_jackknife).
+    Returns (region_ids, bins, group_rows, drop_rows, stats): region ids
+    (group << 32 | HEALPix RING pixel of region_order), the whole catalogue's
+    sums, per-group sums (ascending group id) and for every region the sums of
+    the catalogue without that region's sightlines, all raw XiBin arrays."""
+    L = lib()
+    g = grid.c_struct()
+    flags = XI_EXACT if exact else 0
+    n = C.c_size_t()
+    _check(L.tos_xi_run_jackknife(engine.handle, catalog.handle, C.byref(g), scale, flags, region_order, 0,
+                                  C.byref(n), None, None, None, None, None))
+    nk, nb = n.value, grid.nbins
+    ids = np.zeros(nk, dtype=np.int64)
+    bins = np.zeros(nb, dtype=XIBIN_DTYPE)
+    groups = np.zeros((catalog.num_groups(), nb), dtype=XIBIN_DTYPE)
+    drop = np.zeros((nk, nb), dtype=XIBIN_DTYPE)
+    st = XiStats()
+    _check(L.tos_xi_run_jackknife(engine.handle, catalog.handle, C.byref(g), scale, flags, region_order, nk,
+                                  C.byref(n), _ptr(ids), _ptr(bins), _ptr(groups), _ptr(drop), C.byref(st)))
+    return ids, bins, groups, drop, st.as_dict()
 
 
 def finalize(bins: np.ndarray) -> np.ndarray:

@@ -12,6 +12,9 @@ project; these generators stand in for them:
 * ``small_patch`` — 2,000 sightlines on a 10 x 10 degree patch.
 * ``full_survey`` — 160,000 sightlines (16 per deg^2) over the union of the
   HEALPix nside=8 cells whose centres lie in a seeded ~10,000 deg^2 cap.
+* ``mock_batch`` — mock catalogues with sightline counts log-uniform in
+  [2k, 40k], each on its own seeded cap at 16 sightlines per deg^2, merged
+  into one catalogue with one sightline group per mock (``merge_groups``).
 * ``grf_grid`` — 64^3 Gaussian random field with P(k) ~ k^-2 on a 256 Mpc/h
   periodic box, unit variance, points at cell centres, w = 1.
 """
@@ -165,9 +168,10 @@ def survey_mask(seed: int, area_deg2: float = 10000.0):
     return np.nonzero(cv @ v >= math.cos(cap))[0], v, cap
 
 
-def _ang2pix_ring_nside8(theta: np.ndarray, phi: np.ndarray) -> np.ndarray:
-    """Vectorised RING ang2pix for nside = 8 (Gorski et al. 2005 formulas)."""
-    nside = 8
+def ang2pix_ring(nside: int, theta: np.ndarray, phi: np.ndarray) -> np.ndarray:
+    """Vectorised RING ang2pix (Gorski et al. 2005 formulas)."""
+    theta = np.asarray(theta, dtype=np.float64)
+    phi = np.asarray(phi, dtype=np.float64)
     z = np.cos(theta)
     za = np.abs(z)
     tt = np.mod(phi * (2 / math.pi), 4.0)
@@ -219,7 +223,7 @@ def full_survey(n: int = 160000, seed: int = 7, area_deg2: float = 10000.0, **kw
              + (sz * np.sin(az))[:, None] * e2[None, :])
         th = np.arccos(np.clip(p[:, 2], -1, 1))
         ph = np.mod(np.arctan2(p[:, 1], p[:, 0]), 2 * math.pi)
-        ok = keep[_ang2pix_ring_nside8(th, ph)]
+        ok = keep[ang2pix_ring(8, th, ph)]
         th, ph = th[ok], ph[ok]
         take = min(len(th), n - got)
         ra_out.append(ph[:take])
@@ -228,6 +232,64 @@ def full_survey(n: int = 160000, seed: int = 7, area_deg2: float = 10000.0, **kw
     ra = np.concatenate(ra_out)
     dec = np.concatenate(dec_out)
     return forest_catalog(ra, dec, seed + 2000, **kw)
+
+
+def cap_patch(n: int, seed: int, area_deg2: float, **kw):
+    """n sightlines uniform in a spherical cap of the given area around a
+    seeded random centre."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=3)
+    v /= np.linalg.norm(v)
+    cap = math.acos(max(-1.0, 1.0 - area_deg2 * (math.pi / 180.0) ** 2 / (2 * math.pi)))
+    a = np.array([1.0, 0, 0]) if abs(v[0]) < 0.9 else np.array([0, 1.0, 0])
+    e1 = np.cross(v, a)
+    e1 /= np.linalg.norm(e1)
+    e2 = np.cross(v, e1)
+    cz = rng.uniform(math.cos(cap), 1.0, n)
+    az = rng.uniform(0, 2 * math.pi, n)
+    sz = np.sqrt(1 - cz * cz)
+    p = (cz[:, None] * v[None, :] + (sz * np.cos(az))[:, None] * e1[None, :]
+         + (sz * np.sin(az))[:, None] * e2[None, :])
+    dec = np.arcsin(np.clip(p[:, 2], -1, 1))
+    ra = np.mod(np.arctan2(p[:, 1], p[:, 0]), 2 * math.pi)
+    return forest_catalog(ra, dec, seed + 3000, **kw)
+
+
+def merge_groups(parts):
+    """One batched catalogue from a list of (sightlines, pixels): part k's
+    sightlines get group k and pixel offsets past the earlier parts' pixels."""
+    los_all, px_all, off = [], [], 0
+    for k, (los, px) in enumerate(parts):
+        lk = los.copy()
+        lk["group"] = k
+        lk["pixel_offset"] += np.uint64(off)
+        los_all.append(lk)
+        px_all.append(px)
+        off += len(px)
+    return np.concatenate(los_all), np.concatenate(px_all)
+
+
+def mock_counts(n_mocks: int = 256, seed: int = 11, n_range=(2000, 40000)) -> np.ndarray:
+    """Seeded sightline counts log-uniform in n_range."""
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log(n_range[0]), math.log(n_range[1])
+    return np.exp(rng.uniform(lo, hi, n_mocks)).astype(np.int64)
+
+
+def mock_batch(n_mocks: int = 256, seed: int = 11, n_range=(2000, 40000), density: float = 16.0,
+               first: int = 0, **kw):
+    """Mocks first .. first+n_mocks-1 of the seeded draw of mock_counts(seed):
+    each on its own cap of area count/density deg^2 (seed seed*1000 + k).
+    Returns (parts, scale): parts a list of (sightlines, pixels) and the
+    smallest per-mock scale (every mock with a quasar below z = 2.46 reaches
+    the 3600 A clip, so the scales agree)."""
+    counts = mock_counts(first + n_mocks, seed, n_range)[first:]
+    parts, scale = [], None
+    for k, n in enumerate(counts):
+        los, px, meta = cap_patch(int(n), seed * 1000 + first + k, float(n) / density, **kw)
+        parts.append((los, px))
+        scale = meta["scale"] if scale is None else min(scale, meta["scale"])
+    return parts, scale
 
 
 def grf_grid(n: int = 64, box: float = 256.0, seed: int = 3, index: float = -2.0) -> np.ndarray:
