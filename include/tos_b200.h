@@ -248,6 +248,58 @@ tos_status tos_xi_run_jackknife(tos_engine* engine, tos_catalog* catalog, const 
 /* XiBin::finalize (types.h:96-101) applied to n bins in place. */
 void tos_xibin_finalize(tos_xibin* bins, size_t n);
 
+/* ---- serving: continuous admission of xi requests ------------------------ */
+
+/* A request server on one device.  No counterpart in the reference (which
+ * runs one XiEstimator per process): it serves pair counts of resident
+ * catalogues to many callers.  `slots` worker slots each own a stream and a
+ * workspace and run one request at a time, so requests on different slots
+ * overlap on the device.  A submitted request waits in arrival order until a
+ * slot is free and its workspace fits in memory_budget_bytes beside the
+ * attached catalogues and the other slots' workspaces; idle slots give their
+ * workspaces back when the next request needs the room.  Results equal
+ * tos_xi_run's on the same catalogue, bit for bit (the fixed-point sums do
+ * not depend on the order of the pairs).  The workspace of a request is an
+ * estimate made at submission (exact sizes, sightline pairs estimated for a
+ * uniform sky density with a 1.5 margin). */
+typedef struct tos_server tos_server;
+
+typedef struct {
+  double submit_s, start_s, end_s; /* seconds since the server was created */
+  int32_t slot;                    /* slot that ran the request */
+  int32_t reserved;
+  uint64_t workspace_bytes;        /* workspace estimate used for admission */
+} tos_request_info;
+
+typedef struct {
+  uint64_t budget_bytes, resident_bytes, in_use_bytes, peak_bytes;
+  uint64_t queued, running, completed;
+  uint32_t slots, reserved;
+} tos_server_status;
+
+tos_status tos_server_create(int device, int slots, uint64_t memory_budget_bytes, tos_server** out);
+/* Finishes running requests; queued ones end with TOS_ERR_INVALID_ARG. */
+void tos_server_destroy(tos_server* server);
+/* Count a resident catalogue (created on the server's device with
+ * tos_catalog_create) against the budget; TOS_ERR_OOM when it does not fit.
+ * The catalogue must outlive its requests; detach it before destroying it. */
+tos_status tos_server_attach(tos_server* server, tos_catalog* catalog);
+tos_status tos_server_detach(tos_server* server, tos_catalog* catalog);
+/* Queue tos_xi_run(catalog, grid, scale, flags) without blocking.  flags as
+ * tos_xi_run; TOS_ERR_OOM when the request can never fit in the budget. */
+tos_status tos_server_submit(tos_server* server, tos_catalog* catalog, const tos_grid* grid,
+                             double scale, uint32_t flags, uint64_t* request_id);
+/* Block until the request is done and take its results (then the id is
+ * released): out_bins n_bins sums, out_rows the per-cell or per-group rows
+ * its flags ask for (NULL to drop them), stats and info optional. */
+tos_status tos_server_wait(tos_server* server, uint64_t request_id, tos_xibin* out_bins,
+                           tos_xibin* out_rows, tos_xi_stats* stats, tos_request_info* info);
+tos_status tos_server_status_get(tos_server* server, tos_server_status* out);
+
+/* Device bytes held by a catalogue (its data and the workspace of its own
+ * tos_xi_run calls). */
+tos_status tos_catalog_device_bytes(const tos_catalog* catalog, uint64_t* bytes);
+
 /* ---- brute-force cubic-grid estimator ------------------------------------ */
 
 /* All-pairs isotropic xi(r) of bruteGPU (gpu/brute.cu:63-225) without its

@@ -190,8 +190,8 @@ tos_status sample_covariance(tos_engine* e, double* dX, const double* dw, uint32
 
 tos_status check_last_run(tos_engine* e, tos_catalog* cat) {
   if (!e || !cat) return fail(TOS_ERR_INVALID_ARG, "null argument");
-  if (cat->eng != e) return fail(TOS_ERR_INVALID_ARG, "catalogue belongs to another engine");
-  if (!cat->last_valid || !cat->d_acc.p)
+  if (cat->device != e->device) return fail(TOS_ERR_INVALID_ARG, "catalogue is on another device");
+  if (!cat->run.last_valid || !cat->run.d_acc.p)
     return fail(TOS_ERR_INVALID_ARG, "no completed tos_xi_run on this catalogue");
   return TOS_OK;
 }
@@ -203,16 +203,18 @@ using namespace tos;
 
 extern "C" tos_status tos_xi_cell_covariance(tos_engine* e, tos_catalog* cat, double* mean,
                                              double* cov, double* total_weight) {
+  if (!cat) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> run_lock(cat->run_mu);  // the sums of cat->run stay put
   TOS_TRY(check_last_run(e, cat));
   if (!cov) return fail(TOS_ERR_INVALID_ARG, "cov is null");
   std::lock_guard<std::mutex> lock(e->mu);
   DevGuard g(e->device);
-  const uint32_t nb = cat->last_nb, nc = (uint32_t)cat->cells.size();
+  const uint32_t nb = cat->run.last_nb, nc = (uint32_t)cat->cells.size();
   cudaStream_t st = e->stream;
   DevBuf<double> dX, dw;
   TOS_TRY(dX.alloc((size_t)nc * nb));
   TOS_TRY(dw.alloc(nc));
-  k_cell_samples<<<nc, 256, 0, st>>>(cat->d_acc.p, nb, cat->last_inv_scale[0], cat->last_inv_scale[3],
+  k_cell_samples<<<nc, 256, 0, st>>>(cat->run.d_acc.p, nb, cat->run.last_inv_scale[0], cat->run.last_inv_scale[3],
                                      dX.p, dw.p);
   TOS_CUDA_TRY(cudaGetLastError());
   std::vector<double> w(nc);
@@ -228,6 +230,8 @@ extern "C" tos_status tos_xi_cell_covariance(tos_engine* e, tos_catalog* cat, do
 extern "C" tos_status tos_xi_jackknife(tos_engine* e, tos_catalog* cat, int region_order, size_t cap,
                                        size_t* n_regions, int64_t* region_ids, double* xi_jk,
                                        double* cov) {
+  if (!cat) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> run_lock(cat->run_mu);  // the sums of cat->run stay put
   TOS_TRY(check_last_run(e, cat));
   if (!n_regions) return fail(TOS_ERR_INVALID_ARG, "n_regions is null");
   if (region_order < 0 || region_order > cat->order)
@@ -264,7 +268,7 @@ extern "C" tos_status tos_xi_jackknife(tos_engine* e, tos_catalog* cat, int regi
   std::copy(ids.begin(), ids.end(), region_ids);
   std::lock_guard<std::mutex> lock(e->mu);
   DevGuard g(e->device);
-  const uint32_t nb = cat->last_nb;
+  const uint32_t nb = cat->run.last_nb;
   cudaStream_t st = e->stream;
   DevBuf<__int128> dtot;
   DevBuf<uint32_t> dstart, dmem;
@@ -275,10 +279,10 @@ extern "C" tos_status tos_xi_jackknife(tos_engine* e, tos_catalog* cat, int regi
   TOS_TRY(dX.alloc((size_t)nr * nb));
   TOS_CUDA_TRY(cudaMemcpyAsync(dstart.p, start.data(), (nr + 1) * 4, cudaMemcpyHostToDevice, st));
   TOS_CUDA_TRY(cudaMemcpyAsync(dmem.p, members.data(), nc * 4, cudaMemcpyHostToDevice, st));
-  k_total<<<blocks_for(nb, 128, e->num_sms), 128, 0, st>>>(cat->d_acc.p, (uint32_t)nc, nb, dtot.p);
+  k_total<<<blocks_for(nb, 128, e->num_sms), 128, 0, st>>>(cat->run.d_acc.p, (uint32_t)nc, nb, dtot.p);
   k_region_xi<<<blocks_for((size_t)nr * nb, 128, e->num_sms), 128, 0, st>>>(
-      cat->d_acc.p, nb, dtot.p, dstart.p, dmem.p, (uint32_t)nr, cat->last_inv_scale[0],
-      cat->last_inv_scale[3], dX.p);
+      cat->run.d_acc.p, nb, dtot.p, dstart.p, dmem.p, (uint32_t)nr, cat->run.last_inv_scale[0],
+      cat->run.last_inv_scale[3], dX.p);
   TOS_CUDA_TRY(cudaGetLastError());
   TOS_CUDA_TRY(cudaMemcpyAsync(xi_jk, dX.p, (size_t)nr * nb * 8, cudaMemcpyDeviceToHost, st));
   // C = (N - 1)/N sum_k (xi_k - mean)(xi_k - mean)^T

@@ -542,6 +542,7 @@ __global__ void k_grid_table(const float* U, int ng, const float* thr, int nk, u
 // padded coordinate array and the per-sightline grid offsets.  Grids of more
 // than 65535 values are not used.
 tos_status ensure_grid(tos_engine* e, tos_catalog* cat, int w, cudaStream_t st) {
+  std::lock_guard<std::mutex> lock(cat->grid_mu);
   if (cat->grid_built[w]) return TOS_OK;
   const float* x = (w == 0) ? cat->d_dist_pad.p : cat->d_loglam_pad.p;
   const size_t n = (w == 0) ? cat->d_dist_pad.n : cat->d_loglam_pad.n;
@@ -856,6 +857,12 @@ tos_status tos_catalog_cells(const tos_catalog* c, int64_t* ids, size_t cap) {
   return TOS_OK;
 }
 
+tos_status tos_catalog_device_bytes(const tos_catalog* c, uint64_t* bytes) {
+  if (!c || !bytes) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  *bytes = catalog_data_bytes(c) + c->run.bytes();
+  return TOS_OK;
+}
+
 tos_status tos_catalog_num_groups(const tos_catalog* c, size_t* n) {
   if (!c || !n) return fail(TOS_ERR_INVALID_ARG, "null argument");
   *n = c->groups.size();
@@ -904,12 +911,29 @@ void tos_xibin_finalize(tos_xibin* b, size_t n) {
 
 namespace tos {
 
-tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, double scale,
-                       uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
+uint64_t catalog_data_bytes(const tos_catalog* c) {
+  uint64_t b = c->d_trig.bytes() + c->d_cap.bytes() + c->d_cell_grange.bytes() +
+               c->d_group_cell_start.bytes() + c->d_cell_idx.bytes() + c->d_cell_start.bytes() +
+               c->d_members.bytes() + c->d_npix.bytes() + c->d_off.bytes() + c->d_raw.bytes() +
+               c->d_dist_pad.bytes() + c->d_loglam_pad.bytes() + c->d_wd.bytes() + c->d_w.bytes() +
+               c->d_prefix.bytes() + c->d_range.bytes() + c->d_flags.bytes() + c->d_maxes.bytes();
+  for (int w = 0; w < 2; ++w) b += c->d_grid[w].bytes() + c->d_gfirst[w].bytes();
+  return b;
+}
+
+size_t Workspace::bytes() const {
+  return d_nb_count.bytes() + d_nb_start.bytes() + d_nb.bytes() + d_cnt.bytes() + d_cand.bytes() +
+         d_item_off.bytes() + d_item_i.bytes() + d_item_j.bytes() + d_item_sep.bytes() +
+         d_item_c.bytes() + d_cell_pairs.bytes() + d_acc.bytes() + d_out.bytes() +
+         d_counters.bytes() + d_thr.bytes() + d_gq.bytes() + d_cub_tmp.bytes();
+}
+
+tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos_grid* grid,
+                       double scale, uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
                        tos_xibin* out_cells, tos_xi_stats* stats) {
   const auto t_start = std::chrono::steady_clock::now();
-  if (!e || !cat || !out_bins) return fail(TOS_ERR_INVALID_ARG, "null argument");
-  if (cat->eng != e) return fail(TOS_ERR_INVALID_ARG, "catalogue belongs to another engine");
+  if (!e || !cat || !ws || !out_bins) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (cat->device != e->device) return fail(TOS_ERR_INVALID_ARG, "catalogue is on another device");
   TOS_TRY(check_grid(grid));
   if ((flags & TOS_XI_SUBSAMPLES) && !out_cells)
     return fail(TOS_ERR_INVALID_ARG, "TOS_XI_SUBSAMPLES needs out_cells");
@@ -922,7 +946,7 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
   std::lock_guard<std::mutex> lock(e->mu);
   DeviceGuard dg(e->device);
   cudaStream_t st = e->stream;
-  cat->last_valid = false;
+  ws->last_valid = false;
   const tos_grid& G = *grid;
   const RefGrid rg = make_ref_grid(G);
   {
@@ -945,68 +969,68 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
   const double cos_max = std::cos(max_ang);  // XiEstimator.cc:25
 
   // --- cell neighbours
-  TOS_TRY(cat->d_nb_count.alloc(nc));
-  TOS_TRY(cat->d_nb_start.alloc(nc + 1));
+  TOS_TRY(ws->d_nb_count.alloc(nc));
+  TOS_TRY(ws->d_nb_start.alloc(nc + 1));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[0], st));
   {
     const int gb = grid_for(e, nc, 128);
     k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, cat->d_cell_grange.p, nc, max_ang,
-                                          nullptr, cat->d_nb_count.p, nullptr);
+                                          nullptr, ws->d_nb_count.p, nullptr);
     TOS_CUDA_TRY(cudaGetLastError());
     std::vector<uint32_t> nbc(nc), nbs(nc + 1, 0);
-    TOS_CUDA_TRY(cudaMemcpyAsync(nbc.data(), cat->d_nb_count.p, nc * 4, cudaMemcpyDeviceToHost, st));
+    TOS_CUDA_TRY(cudaMemcpyAsync(nbc.data(), ws->d_nb_count.p, nc * 4, cudaMemcpyDeviceToHost, st));
     TOS_CUDA_TRY(cudaStreamSynchronize(st));
     for (uint32_t c = 0; c < nc; ++c) nbs[c + 1] = nbs[c] + nbc[c];
-    TOS_TRY(cat->d_nb.alloc(nbs[nc]));
-    TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_nb_start.p, nbs.data(), (nc + 1) * 4,
+    TOS_TRY(ws->d_nb.alloc(nbs[nc]));
+    TOS_CUDA_TRY(cudaMemcpyAsync(ws->d_nb_start.p, nbs.data(), (nc + 1) * 4,
                                  cudaMemcpyHostToDevice, st));
     k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, cat->d_cell_grange.p, nc, max_ang,
-                                          cat->d_nb_start.p, nullptr, cat->d_nb.p);
+                                          ws->d_nb_start.p, nullptr, ws->d_nb.p);
     TOS_CUDA_TRY(cudaGetLastError());
   }
   // --- expansion pass 1: counts
   const uint32_t nm = (uint32_t)cat->n_los;
-  TOS_TRY(cat->d_cnt.alloc(nm));
-  TOS_TRY(cat->d_cand.alloc(nm));
-  TOS_TRY(cat->d_item_off.alloc(nm));
-  TOS_TRY(cat->d_cell_pairs.alloc(nc));
-  TOS_TRY(cat->d_counters.alloc(4200));
-  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_cell_pairs.p, 0, nc * 8, st));
-  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_counters.p, 0, 4200 * 8, st));
+  TOS_TRY(ws->d_cnt.alloc(nm));
+  TOS_TRY(ws->d_cand.alloc(nm));
+  TOS_TRY(ws->d_item_off.alloc(nm));
+  TOS_TRY(ws->d_cell_pairs.alloc(nc));
+  TOS_TRY(ws->d_counters.alloc(4200));
+  TOS_CUDA_TRY(cudaMemsetAsync(ws->d_cell_pairs.p, 0, nc * 8, st));
+  TOS_CUDA_TRY(cudaMemsetAsync(ws->d_counters.p, 0, 4200 * 8, st));
   // [0..3] kernel counters, [4] pair-kernel item counter, [5] candidates,
   // [6] window flushes, [7] run-kernel item counter, [8] run items, [9] grid
   // items, [10] grid-kernel item counter,
   // [16] theta indices on an edge, [17..] their item numbers (4096 at most)
-  unsigned long long* ctr = cat->d_counters.p;
+  unsigned long long* ctr = ws->d_counters.p;
   const double theta_min = G.axis[1].min, theta_inv = 1.0 / axis_width(G.axis[1]);
   const int ge = grid_for(e, (size_t)nm * 32, 256);
   k_expand<<<ge, 256, 0, st>>>(cat->d_members.p, nm, cat->d_cell_idx.p, cat->d_cell_start.p,
-                               cat->d_nb_start.p, cat->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
-                               cat->d_cnt.p, cat->d_cand.p, cat->d_cell_pairs.p, nullptr, nullptr,
+                               ws->d_nb_start.p, ws->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
+                               ws->d_cnt.p, ws->d_cand.p, ws->d_cell_pairs.p, nullptr, nullptr,
                                nullptr, nullptr, nullptr, G.type, theta_min, theta_inv, ctr + 16);
   TOS_CUDA_TRY(cudaGetLastError());
   // exclusive scan of counts -> item offsets
   size_t tmp_bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cat->d_cnt.p, cat->d_item_off.p, nm, st);
-  TOS_TRY(cat->d_cub_tmp.alloc(tmp_bytes + 16));
-  TOS_CUDA_TRY(cub::DeviceScan::ExclusiveSum(cat->d_cub_tmp.p, tmp_bytes, cat->d_cnt.p,
-                                             cat->d_item_off.p, nm, st));
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, ws->d_cnt.p, ws->d_item_off.p, nm, st);
+  TOS_TRY(ws->d_cub_tmp.alloc(tmp_bytes + 16));
+  TOS_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ws->d_cub_tmp.p, tmp_bytes, ws->d_cnt.p,
+                                             ws->d_item_off.p, nm, st));
   uint32_t last_off = 0, last_cnt = 0;
-  TOS_CUDA_TRY(cudaMemcpyAsync(&last_off, cat->d_item_off.p + nm - 1, 4, cudaMemcpyDeviceToHost, st));
-  TOS_CUDA_TRY(cudaMemcpyAsync(&last_cnt, cat->d_cnt.p + nm - 1, 4, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(&last_off, ws->d_item_off.p + nm - 1, 4, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(&last_cnt, ws->d_cnt.p + nm - 1, 4, cudaMemcpyDeviceToHost, st));
   std::vector<unsigned long long> cell_pairs(nc);
-  TOS_CUDA_TRY(cudaMemcpyAsync(cell_pairs.data(), cat->d_cell_pairs.p, nc * 8,
+  TOS_CUDA_TRY(cudaMemcpyAsync(cell_pairs.data(), ws->d_cell_pairs.p, nc * 8,
                                cudaMemcpyDeviceToHost, st));
   unsigned long long n_cand_total = 0;
   {
     // candidates: reduce on the device
     size_t tb = 0;
-    cub::DeviceReduce::Sum(nullptr, tb, cat->d_cand.p, ctr + 5, nm, st);
-    if (tb > cat->d_cub_tmp.n) {
+    cub::DeviceReduce::Sum(nullptr, tb, ws->d_cand.p, ctr + 5, nm, st);
+    if (tb > ws->d_cub_tmp.n) {
       TOS_CUDA_TRY(cudaStreamSynchronize(st));
-      TOS_TRY(cat->d_cub_tmp.alloc(tb + 16));
+      TOS_TRY(ws->d_cub_tmp.alloc(tb + 16));
     }
-    TOS_CUDA_TRY(cub::DeviceReduce::Sum(cat->d_cub_tmp.p, tb, cat->d_cand.p, ctr + 5, nm, st));
+    TOS_CUDA_TRY(cub::DeviceReduce::Sum(ws->d_cub_tmp.p, tb, ws->d_cand.p, ctr + 5, nm, st));
     TOS_CUDA_TRY(cudaMemcpyAsync(&n_cand_total, ctr + 5, 8, cudaMemcpyDeviceToHost, st));
   }
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1017,15 +1041,15 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
     max_cell_pairs = std::max(max_cell_pairs, v);
   }
   // --- expansion pass 2: items
-  TOS_TRY(cat->d_item_i.alloc(n_items));
-  TOS_TRY(cat->d_item_j.alloc(n_items));
-  TOS_TRY(cat->d_item_c.alloc(n_items));
-  TOS_TRY(cat->d_item_sep.alloc(G.type == TOS_OBSERVING ? n_items : 1));
+  TOS_TRY(ws->d_item_i.alloc(n_items));
+  TOS_TRY(ws->d_item_j.alloc(n_items));
+  TOS_TRY(ws->d_item_c.alloc(n_items));
+  TOS_TRY(ws->d_item_sep.alloc(G.type == TOS_OBSERVING ? n_items : 1));
   k_expand<<<ge, 256, 0, st>>>(cat->d_members.p, nm, cat->d_cell_idx.p, cat->d_cell_start.p,
-                               cat->d_nb_start.p, cat->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
-                               cat->d_cnt.p, cat->d_cand.p, cat->d_cell_pairs.p, cat->d_item_off.p,
-                               cat->d_item_i.p, cat->d_item_j.p, cat->d_item_c.p,
-                               cat->d_item_sep.p, G.type, theta_min, theta_inv, ctr + 16);
+                               ws->d_nb_start.p, ws->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
+                               ws->d_cnt.p, ws->d_cand.p, ws->d_cell_pairs.p, ws->d_item_off.p,
+                               ws->d_item_i.p, ws->d_item_j.p, ws->d_item_c.p,
+                               ws->d_item_sep.p, G.type, theta_min, theta_inv, ctr + 16);
   TOS_CUDA_TRY(cudaGetLastError());
   if (G.type == TOS_OBSERVING) {
     // theta indices within 1e-9 of an edge: recompute with the host libm acos,
@@ -1039,9 +1063,9 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
       TOS_CUDA_TRY(cudaMemcpy(at.data(), ctr + 17, nflag * 8, cudaMemcpyDeviceToHost));
       for (auto a : at) {
         double c;
-        TOS_CUDA_TRY(cudaMemcpy(&c, cat->d_item_c.p + a, 8, cudaMemcpyDeviceToHost));
+        TOS_CUDA_TRY(cudaMemcpy(&c, ws->d_item_c.p + a, 8, cudaMemcpyDeviceToHost));
         const uint32_t sep = tos::ref_u32(tos::dmul(tos::dsub(std::acos(c), theta_min), theta_inv));
-        TOS_CUDA_TRY(cudaMemcpy(cat->d_item_sep.p + a, &sep, 4, cudaMemcpyHostToDevice));
+        TOS_CUDA_TRY(cudaMemcpy(ws->d_item_sep.p + a, &sep, 4, cudaMemcpyHostToDevice));
       }
     }
   }
@@ -1050,8 +1074,8 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
   // --- accumulation layout and fixed-point scales
   const size_t n_acc_rows = plan ? (size_t)plan->n_rows : (size_t)nc;
   const size_t acc_words = n_acc_rows * nb * kAccWords;
-  TOS_TRY(cat->d_acc.alloc(acc_words));
-  TOS_CUDA_TRY(cudaMemsetAsync(cat->d_acc.p, 0, acc_words * 8, st));
+  TOS_TRY(ws->d_acc.alloc(acc_words));
+  TOS_CUDA_TRY(cudaMemsetAsync(ws->d_acc.p, 0, acc_words * 8, st));
   PairArgs A{};
   A.off = cat->d_off.p;
   A.npix = cat->d_npix.p;
@@ -1068,14 +1092,14 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
     A.slot_key = plan->slot_key;
     A.spill_row = plan->n_rows - 1;
   }
-  A.item_i = cat->d_item_i.p;
-  A.item_j = cat->d_item_j.p;
-  A.item_c = cat->d_item_c.p;
-  A.item_sep = cat->d_item_sep.p;
+  A.item_i = ws->d_item_i.p;
+  A.item_j = ws->d_item_j.p;
+  A.item_c = ws->d_item_c.p;
+  A.item_sep = ws->d_item_sep.p;
   A.n_items = n_items;
   A.next_item = ctr + 4;
   A.g = rg;
-  A.acc = cat->d_acc.p;
+  A.acc = ws->d_acc.p;
   A.counters = ctr;
   A.force_exact = (flags & TOS_XI_EXACT) ? 1 : 0;
   // fixed point: 2^F per field.  A run contributes c with |c| <= bound
@@ -1196,10 +1220,10 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
       }
     }
     if (use_runs) {
-      TOS_TRY(cat->d_thr.alloc(n0 + 1));
-      TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_thr.p, thr.data(), (n0 + 1) * sizeof(float),
+      TOS_TRY(ws->d_thr.alloc(n0 + 1));
+      TOS_CUDA_TRY(cudaMemcpyAsync(ws->d_thr.p, thr.data(), (n0 + 1) * sizeof(float),
                                    cudaMemcpyHostToDevice, st));
-      A.thr = cat->d_thr.p;
+      A.thr = ws->d_thr.p;
       // one FP64 register sum can hold a whole item's pairs of a bin
       // (at most max_np^2): every field takes the wide 62-bit conversion
       const double m = std::max<double>(1.0, cat->max_np);
@@ -1224,11 +1248,11 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
     const int ng = cat->grid_n[w];
     if (ng > 0 && cat->grid_los[w] > 0) {
       const size_t nq = (size_t)2 * ng * (n0 + 1);
-      TOS_TRY(cat->d_gq.alloc(nq));
-      k_grid_table<<<grid_for(e, nq, 256), 256, 0, st>>>(cat->d_grid[w].p, ng, cat->d_thr.p,
-                                                         (int)n0 + 1, cat->d_gq.p);
+      TOS_TRY(ws->d_gq.alloc(nq));
+      k_grid_table<<<grid_for(e, nq, 256), 256, 0, st>>>(cat->d_grid[w].p, ng, ws->d_thr.p,
+                                                         (int)n0 + 1, ws->d_gq.p);
       TOS_CUDA_TRY(cudaGetLastError());
-      A.gq = cat->d_gq.p;
+      A.gq = ws->d_gq.p;
       A.gfirst = cat->d_gfirst[w].p;
       A.ng = ng;
       A.grid_split = 1;
@@ -1268,36 +1292,36 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, do
   const bool per_group = (flags & TOS_XI_PER_GROUP) != 0;
   const uint32_t ngr = (uint32_t)cat->groups.size();
   const size_t n_rows = want_cells ? (size_t)nc : per_group ? (size_t)ngr : 0;
-  TOS_TRY(cat->d_out.alloc((size_t)nb * (n_rows + 1)));
+  TOS_TRY(ws->d_out.alloc((size_t)nb * (n_rows + 1)));
   double4 ia, ib;
   ia.x = 1.0 / A.scale[0], ia.y = 1.0 / A.scale[1], ia.z = 1.0 / A.scale[2], ia.w = 1.0 / A.scale[3];
   ib.x = 1.0 / A.scale[4], ib.y = 1.0 / A.scale[5], ib.z = 1.0 / A.scale[6], ib.w = 0;
   if (plan) {
     double inv[7];
     for (int k = 0; k < 7; ++k) inv[k] = 1.0 / A.scale[k];
-    TOS_TRY(plan->combine(st, nb, inv, cat->d_out.p));
+    TOS_TRY(plan->combine(st, nb, inv, ws->d_acc.p, ws->d_out.p));
   } else if (per_group) {
     k_combine_groups<<<grid_for(e, (size_t)ngr * nb, 128), 128, 0, st>>>(
-        cat->d_acc.p, cat->d_group_cell_start.p, ngr, nb, ia, ib, cat->d_out.p + nb);
+        ws->d_acc.p, cat->d_group_cell_start.p, ngr, nb, ia, ib, ws->d_out.p + nb);
     TOS_CUDA_TRY(cudaGetLastError());
-    launch_sum_rows(cat->d_out.p + nb, ngr, nb, cat->d_out.p, grid_for(e, nb, 128), st);
+    launch_sum_rows(ws->d_out.p + nb, ngr, nb, ws->d_out.p, grid_for(e, nb, 128), st);
   } else {
-    k_combine<<<grid_for(e, nb, 128), 128, 0, st>>>(cat->d_acc.p, nc, nb, ia, ib, cat->d_out.p,
-                                                     want_cells ? cat->d_out.p + nb : nullptr);
+    k_combine<<<grid_for(e, nb, 128), 128, 0, st>>>(ws->d_acc.p, nc, nb, ia, ib, ws->d_out.p,
+                                                     want_cells ? ws->d_out.p + nb : nullptr);
   }
   TOS_CUDA_TRY(cudaGetLastError());
-  TOS_CUDA_TRY(cudaMemcpyAsync(out_bins, cat->d_out.p, (size_t)nb * sizeof(tos_xibin),
+  TOS_CUDA_TRY(cudaMemcpyAsync(out_bins, ws->d_out.p, (size_t)nb * sizeof(tos_xibin),
                                cudaMemcpyDeviceToHost, st));
   if (n_rows)
-    TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, cat->d_out.p + nb, n_rows * nb * sizeof(tos_xibin),
+    TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, ws->d_out.p + nb, n_rows * nb * sizeof(tos_xibin),
                                  cudaMemcpyDeviceToHost, st));
   unsigned long long hc[10];
   TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
-  cat->last_valid = (plan == nullptr);  // slot rows are not per-cell sums
-  cat->last_nb = nb;
-  for (int k = 0; k < 7; ++k) cat->last_inv_scale[k] = 1.0 / A.scale[k];
+  ws->last_valid = (plan == nullptr);  // slot rows are not per-cell sums
+  ws->last_nb = nb;
+  for (int k = 0; k < 7; ++k) ws->last_inv_scale[k] = 1.0 / A.scale[k];
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->num_sightlines = cat->n_los;
@@ -1342,7 +1366,9 @@ extern "C" {
 tos_status tos_xi_run(tos_engine* e, tos_catalog* cat, const tos_grid* grid, double scale,
                       uint32_t flags, tos_xibin* out_bins, tos_xibin* out_cells,
                       tos_xi_stats* stats) {
-  return xi_run_impl(e, cat, grid, scale, flags, nullptr, out_bins, out_cells, stats);
+  if (!cat) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lock(cat->run_mu);
+  return xi_run_impl(e, cat, &cat->run, grid, scale, flags, nullptr, out_bins, out_cells, stats);
 }
 
 }  // extern "C"

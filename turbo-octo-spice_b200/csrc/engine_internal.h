@@ -58,6 +58,36 @@ struct DevBuf {
     n = count;
     return TOS_OK;
   }
+  size_t bytes() const { return p ? n * sizeof(T) : 0; }
+};
+
+}  // namespace tos
+
+namespace tos {
+
+// Device scratch of one pair count, kept between runs so that a caller that
+// runs again (a server slot, the catalogue's own runs) allocates only when a
+// run needs more than before.
+struct Workspace {
+  DevBuf<uint32_t> d_nb_count, d_nb_start, d_nb;  // cell neighbour CSR
+  DevBuf<uint32_t> d_cnt;                         // per primary: accepted pairs
+  DevBuf<unsigned long long> d_cand;              // per primary candidates (for stats)
+  DevBuf<uint32_t> d_item_off;
+  DevBuf<uint32_t> d_item_i, d_item_j, d_item_sep;
+  DevBuf<double> d_item_c;
+  DevBuf<unsigned long long> d_cell_pairs;        // per cell sum N_i N_j
+  DevBuf<unsigned long long> d_acc;               // [n_rows][n_bins][16] 128-bit fixed point
+  DevBuf<tos_xibin> d_out;                        // combined / per row output
+  DevBuf<unsigned long long> d_counters;          // misc counters
+  DevBuf<float> d_thr;                            // first-axis thresholds of the run sweep
+  DevBuf<uint16_t> d_gq;                          // boundary table of the current call
+  DevBuf<unsigned char> d_cub_tmp;
+  // the last completed per-cell run in d_acc
+  bool last_valid = false;
+  uint32_t last_nb = 0;
+  double last_inv_scale[7] = {};                  // fixed point -> value, per field
+  // bytes held by the buffers above
+  size_t bytes() const;
 };
 
 }  // namespace tos
@@ -110,30 +140,17 @@ struct tos_catalog {
   double min_d = 0;                 // smallest distance
   double min_gap = 0;               // smallest positive distance step within a sightline (lower bound)
   uint32_t max_np = 0;
-  // run scratch (kept between runs)
-  tos::DevBuf<uint32_t> d_nb_count, d_nb_start, d_nb;  // cell neighbour CSR
-  tos::DevBuf<uint32_t> d_cnt;                         // per primary: accepted pairs
-  tos::DevBuf<unsigned long long> d_cand;              // per primary candidates (for stats)
-  tos::DevBuf<uint32_t> d_item_off;
-  tos::DevBuf<uint32_t> d_item_i, d_item_j, d_item_sep;
-  tos::DevBuf<double> d_item_c;
-  tos::DevBuf<unsigned long long> d_cell_pairs;        // per cell sum N_i N_j
-  tos::DevBuf<unsigned long long> d_acc;               // [n_cells][n_bins][16] 128-bit fixed point
-  tos::DevBuf<tos_xibin> d_out;                        // combined / per cell output
-  tos::DevBuf<unsigned long long> d_counters;          // misc counters
-  tos::DevBuf<float> d_thr;                            // first-axis thresholds of the run sweep
   // common first-axis grids (0: distance, 1: loglam), built on first use
+  std::mutex grid_mu;                                  // guards the grid build
   bool grid_built[2] = {false, false};
   int grid_n[2] = {0, 0};                              // distinct values (0: no usable grid)
   uint64_t grid_los[2] = {0, 0};                       // sightlines contiguous on the grid
   tos::DevBuf<float> d_grid[2];                        // sorted distinct values
   tos::DevBuf<uint32_t> d_gfirst[2];                   // per sightline grid index of pixel 0 or kNoGrid
-  tos::DevBuf<uint16_t> d_gq;                          // boundary table of the current call
-  // the last completed tos_xi_run: its per-cell sums stay in d_acc
-  bool last_valid = false;
-  uint32_t last_nb = 0;
-  double last_inv_scale[7] = {};                       // fixed point -> value, per field
-  tos::DevBuf<unsigned char> d_cub_tmp;
+  // the workspace of tos_xi_run on this catalogue; its per-cell sums stay
+  // there after the run for the covariance calls
+  tos::Workspace run;
+  std::mutex run_mu;                                   // one tos_xi_run at a time on `run`
 };
 
 namespace tos {
@@ -148,22 +165,32 @@ struct RowPlan {
   const uint32_t* slot_key = nullptr;
   // enqueues the combine on the stream: writes the nb run totals to
   // d_out[0..nb) and any further outputs; inv_scale converts fixed point
-  std::function<tos_status(cudaStream_t, uint32_t nb, const double* inv_scale, tos_xibin* d_out)>
+  std::function<tos_status(cudaStream_t, uint32_t nb, const double* inv_scale,
+                           const unsigned long long* d_acc, tos_xibin* d_out)>
       combine;
 };
 
-// The pair count behind tos_xi_run: plan = null accumulates per cell (and
+// The pair count behind tos_xi_run, with its scratch in `ws` (the caller
+// owns ws exclusively for the call): plan = null accumulates per cell (and
 // honours TOS_XI_SUBSAMPLES / TOS_XI_PER_GROUP), otherwise into the plan's
-// slots, combined by plan->combine.  Takes the engine lock.
-tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, const tos_grid* grid, double scale,
-                       uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
+// slots, combined by plan->combine.  Takes the engine lock; the catalogue is
+// only read, so runs with different workspaces may share it.
+tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos_grid* grid,
+                       double scale, uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
                        tos_xibin* out_cells, tos_xi_stats* stats);
 
 // out[b] = rows[0][b] + rows[1][b] + ... (n_rows x nb XiBins, ascending row order).
 void launch_sum_rows(const tos_xibin* rows, uint32_t n_rows, uint32_t nb, tos_xibin* out,
                      int blocks, cudaStream_t st);
 
+// Device bytes of a catalogue's own data (not its workspace).
+uint64_t catalog_data_bytes(const tos_catalog* c);
+
 // Maximum angular scale of a grid (the grid classes' maxAngularScale).
 double max_angular_scale(const tos_grid& g, double scale);
 
 }  // namespace tos
+
+// Build (once) the catalogue's common first-axis grid w (0: distance,
+// 1: loglam) for the grid sweep; thread-safe.
+tos_status ensure_grid(tos_engine* e, tos_catalog* cat, int w, cudaStream_t st);

@@ -140,7 +140,7 @@ extern "C" tos_status tos_xi_run_jackknife(tos_engine* e, tos_catalog* cat, cons
                                            tos_xibin* out_bins, tos_xibin* out_groups,
                                            tos_xibin* out_drop, tos_xi_stats* stats) {
   if (!e || !cat || !grid || !n_regions) return fail(TOS_ERR_INVALID_ARG, "null argument");
-  if (cat->eng != e) return fail(TOS_ERR_INVALID_ARG, "catalogue belongs to another engine");
+  if (cat->device != e->device) return fail(TOS_ERR_INVALID_ARG, "catalogue is on another device");
   if (flags & ~TOS_XI_EXACT)
     return fail(TOS_ERR_INVALID_ARG, "a jackknife run takes no flag but TOS_XI_EXACT");
   if (region_order < 0 || region_order > cat->order)
@@ -258,22 +258,22 @@ extern "C" tos_status tos_xi_run_jackknife(tos_engine* e, tos_catalog* cat, cons
   plan.slot_start = d_slot_start.p;
   plan.slot_key = d_slot_key.p;
   plan.combine = [&](cudaStream_t st, uint32_t nb, const double* inv_scale,
-                     tos_xibin* d_out) -> tos_status {
+                     const unsigned long long* d_acc, tos_xibin* d_out) -> tos_status {
     Inv7 inv;
     for (int k = 0; k < 7; ++k) inv.v[k] = inv_scale[k];
     TOS_TRY(d_gtot.alloc((size_t)ngr * nb * kAccWords));
     TOS_TRY(d_gout.alloc((size_t)ngr * nb));
     TOS_TRY(d_drop.alloc((size_t)nk * nb));
     TOS_CUDA_TRY(cudaMemsetAsync(d_spill.p, 0, 8, st));
-    k_group_totals<<<blocks(e, (size_t)ngr * nb), 128, 0, st>>>(cat->d_acc.p, nb, d_gslot.p, ngr, inv,
+    k_group_totals<<<blocks(e, (size_t)ngr * nb), 128, 0, st>>>(d_acc, nb, d_gslot.p, ngr, inv,
                                                                 d_gtot.p, d_gout.p);
     TOS_CUDA_TRY(cudaGetLastError());
     launch_sum_rows(d_gout.p, ngr, nb, d_out, blocks(e, nb), st);
     TOS_CUDA_TRY(cudaGetLastError());
-    k_drop<<<blocks(e, (size_t)nk * nb), 128, 0, st>>>(cat->d_acc.p, d_gtot.p, nb, d_kslot_start.p,
+    k_drop<<<blocks(e, (size_t)nk * nb), 128, 0, st>>>(d_acc, d_gtot.p, nb, d_kslot_start.p,
                                                        d_kslot.p, d_kgroup.p, nk, inv, d_drop.p);
     TOS_CUDA_TRY(cudaGetLastError());
-    k_row_count<<<1, 256, 0, st>>>(cat->d_acc.p + (size_t)ns * nb * kAccWords, nb, d_spill.p);
+    k_row_count<<<1, 256, 0, st>>>(d_acc + (size_t)ns * nb * kAccWords, nb, d_spill.p);
     TOS_CUDA_TRY(cudaGetLastError());
     if (out_groups)
       TOS_CUDA_TRY(cudaMemcpyAsync(out_groups, d_gout.p, (size_t)ngr * nb * sizeof(tos_xibin),
@@ -283,7 +283,10 @@ extern "C" tos_status tos_xi_run_jackknife(tos_engine* e, tos_catalog* cat, cons
     TOS_CUDA_TRY(cudaMemcpyAsync(&spill, d_spill.p, 8, cudaMemcpyDeviceToHost, st));
     return TOS_OK;
   };
-  TOS_TRY(xi_run_impl(e, cat, grid, scale, flags, &plan, out_bins, nullptr, stats));
+  {
+    std::lock_guard<std::mutex> lock(cat->run_mu);
+    TOS_TRY(xi_run_impl(e, cat, &cat->run, grid, scale, flags, &plan, out_bins, nullptr, stats));
+  }
   if (spill != 0)
     return fail(TOS_ERR_INTERNAL, std::to_string(spill) + " pixel pairs found no region slot");
   return TOS_OK;

@@ -1,0 +1,331 @@
+// server.cu — a request server over resident catalogues: continuous
+// admission of xi requests to worker slots under a device-memory budget.
+//
+// Each slot owns an engine (its own stream) and a workspace, and runs one
+// request at a time on a host thread of its own, so the requests of
+// different slots overlap on the device: one slot's kernels run while
+// another is in its host phase (neighbour counts, item offsets) or while
+// its own kernels leave SMs idle.  A request is admitted to a free slot as
+// soon as one frees up and its workspace fits in the budget beside the
+// resident catalogues and the other slots' workspaces (admission.h), in
+// arrival order.  Runs on one catalogue never write to it, so any number of
+// slots may count pairs of the same catalogue at once.  The results are
+// those of tos_xi_run on the same catalogue: the fixed-point sums do not
+// depend on the order in which pairs are added.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <cmath>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "admission.h"
+#include "engine_internal.h"
+
+namespace tos {
+namespace {
+
+struct Request {
+  uint64_t id = 0;
+  tos_catalog* cat = nullptr;
+  tos_grid grid{};
+  double scale = 0;
+  uint32_t flags = 0;
+  uint64_t need = 0;   // workspace estimate (bytes)
+  size_t n_rows = 0;   // per-cell or per-group rows returned
+  std::vector<tos_xibin> bins, rows;
+  tos_xi_stats stats{};
+  tos_status status = TOS_OK;
+  std::string error;
+  tos_request_info info{};
+  bool done = false;
+};
+
+constexpr double kPi = 3.14159265358979323846;
+
+// Device bytes a run of `cat` on grid g needs in a workspace.  The sightline
+// pairs are estimated for a uniform sky density over the occupied cells
+// (pairs ~ N^2 / 2 * disc / area, with a 1.5 margin); the rest is exact.
+uint64_t workspace_estimate(const tos_catalog* cat, const tos_grid& g, double scale, size_t n_rows) {
+  const double nb = (double)g.axis[0].nbins * g.axis[1].nbins * g.axis[2].nbins;
+  const double nc = (double)cat->cells.size(), n = (double)cat->n_los;
+  const double cell_sr = 4.0 * kPi / (12.0 * (double)cat->nside * (double)cat->nside);
+  const double area = std::max(nc * cell_sr, cell_sr);
+  const double ang = std::min(max_angular_scale(g, scale), kPi);
+  const double disc = 2.0 * kPi * (1.0 - std::cos(ang));
+  const double partners = std::min(n, n * disc / area);
+  const double pairs = 1.5 * 0.5 * n * partners + n;
+  const double near_cells = std::min(nc, nc * disc / area + 9.0);
+  double bytes = 0;
+  bytes += nc * nb * 128.0;                                   // per-cell sums
+  bytes += nb * sizeof(tos_xibin) * (1.0 + (double)n_rows);   // results
+  bytes += pairs * 20.0;                                      // items (i, j, cos, theta index)
+  bytes += n * 24.0;                                          // per primary counts and offsets
+  bytes += nc * (near_cells + 12.0) * 4.0;                    // cell neighbours
+  bytes += 4200.0 * 8 + 2.0 * 65536 * (g.axis[0].nbins + 1.0) + 1e6;  // counters, tables, cub
+  return (uint64_t)bytes;
+}
+
+
+}  // namespace
+}  // namespace tos
+
+struct tos_server {
+  explicit tos_server(int slots, uint64_t budget) : adm(slots, budget) {}
+  int device = 0;
+  tos::Admission adm;
+  tos_engine* setup = nullptr;                 // catalogue preparation at attach
+  std::vector<tos_engine*> engines;            // per slot
+  std::vector<std::unique_ptr<tos::Workspace>> ws;
+  std::vector<tos::Request*> assigned;         // per slot: the running request
+  std::vector<std::thread> threads;
+  std::mutex mu;
+  std::condition_variable cv_slot, cv_done;
+  std::deque<tos::Request*> queue;
+  std::unordered_map<uint64_t, std::unique_ptr<tos::Request>> reqs;
+  std::unordered_map<const tos_catalog*, uint64_t> attached;  // catalogue -> resident bytes
+  std::unordered_map<const tos_catalog*, uint64_t> pending;   // unfinished requests per catalogue
+  uint64_t next_id = 1, completed = 0, peak = 0;
+  bool stop = false;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  // Start queued requests while the head fits (mu held).
+  void dispatch() {
+    while (!queue.empty()) {
+      tos::Request* r = queue.front();
+      const int k = adm.pick(r->need);
+      if (k < 0) {
+        const int v = adm.trim_victim(r->need);
+        if (v < 0) break;  // wait for a running request to finish
+        // an idle slot gives its workspace back (its stream has no work)
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        ws[v].reset(new tos::Workspace());
+        cudaSetDevice(prev);
+        adm.release(v);
+        continue;
+      }
+      queue.pop_front();
+      adm.start(k, r->need);
+      peak = std::max(peak, adm.in_use());
+      r->info.start_s = now();
+      r->info.slot = k;
+      assigned[k] = r;
+      cv_slot.notify_all();
+    }
+  }
+
+  void worker(int k) {
+    cudaSetDevice(device);
+    for (;;) {
+      tos::Request* r = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_slot.wait(lk, [&] { return stop || assigned[k] != nullptr; });
+        if (!assigned[k]) return;  // stopped and idle
+        r = assigned[k];
+      }
+      const size_t nb = (size_t)r->grid.axis[0].nbins * r->grid.axis[1].nbins * r->grid.axis[2].nbins;
+      r->bins.assign(nb, tos_xibin{});
+      r->rows.assign(r->n_rows * nb, tos_xibin{});
+      const tos_status s = tos::xi_run_impl(engines[k], r->cat, ws[k].get(), &r->grid, r->scale,
+                                            r->flags, nullptr, r->bins.data(),
+                                            r->n_rows ? r->rows.data() : nullptr, &r->stats);
+      std::string err = (s == TOS_OK) ? std::string() : std::string(tos_last_error());
+      const uint64_t held = ws[k]->bytes();
+      std::lock_guard<std::mutex> lk(mu);
+      r->status = s;
+      r->error = err;
+      r->info.end_s = now();
+      r->done = true;
+      assigned[k] = nullptr;
+      adm.finish(k, held);
+      peak = std::max(peak, adm.in_use());
+      if (--pending[r->cat] == 0) pending.erase(r->cat);
+      ++completed;
+      dispatch();
+      cv_done.notify_all();
+    }
+  }
+};
+
+using namespace tos;
+
+extern "C" {
+
+tos_status tos_server_create(int device, int slots, uint64_t memory_budget_bytes, tos_server** out) {
+  if (!out) return fail(TOS_ERR_INVALID_ARG, "out is null");
+  *out = nullptr;
+  if (slots < 1 || slots > 64) return fail(TOS_ERR_INVALID_ARG, "slots must be in [1, 64]");
+  std::unique_ptr<tos_server> s(new tos_server(slots, memory_budget_bytes));
+  s->device = device;
+  TOS_TRY(tos_engine_create(device, &s->setup));
+  for (int k = 0; k < slots; ++k) {
+    tos_engine* e = nullptr;
+    const tos_status st = tos_engine_create(device, &e);
+    if (st != TOS_OK) {
+      for (tos_engine* x : s->engines) tos_engine_destroy(x);
+      tos_engine_destroy(s->setup);
+      return st;
+    }
+    s->engines.push_back(e);
+    s->ws.emplace_back(new Workspace());
+  }
+  s->assigned.assign(slots, nullptr);
+  for (int k = 0; k < slots; ++k) s->threads.emplace_back(&tos_server::worker, s.get(), k);
+  *out = s.release();
+  return TOS_OK;
+}
+
+void tos_server_destroy(tos_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    for (Request* r : s->queue) {  // never started
+      r->status = TOS_ERR_INVALID_ARG;
+      r->error = "server destroyed before the request started";
+      r->done = true;
+    }
+    s->queue.clear();
+    s->cv_slot.notify_all();
+    s->cv_done.notify_all();
+  }
+  for (auto& t : s->threads) t.join();  // running requests finish first
+  {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->device);
+    s->ws.clear();
+    cudaSetDevice(prev);
+  }
+  for (tos_engine* e : s->engines) tos_engine_destroy(e);
+  tos_engine_destroy(s->setup);
+  delete s;
+}
+
+tos_status tos_server_attach(tos_server* s, tos_catalog* cat) {
+  if (!s || !cat) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (cat->device != s->device) return fail(TOS_ERR_INVALID_ARG, "catalogue is on another device");
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->attached.count(cat)) return TOS_OK;
+  }
+  // the common-grid tables are built once per catalogue, before any request
+  {
+    std::lock_guard<std::mutex> el(s->setup->mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->device);
+    tos_status st = TOS_OK;
+    for (int w = 0; w < 2 && st == TOS_OK; ++w) st = ensure_grid(s->setup, cat, w, s->setup->stream);
+    cudaSetDevice(prev);
+    TOS_TRY(st);
+  }
+  const uint64_t bytes = catalog_data_bytes(cat) + cat->run.bytes();
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->adm.add_resident(bytes))
+    return fail(TOS_ERR_OOM, "catalogue (" + std::to_string(bytes) +
+                                 " bytes) does not fit in the server's memory budget");
+  s->attached[cat] = bytes;
+  return TOS_OK;
+}
+
+tos_status tos_server_detach(tos_server* s, tos_catalog* cat) {
+  if (!s || !cat) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->attached.find(cat);
+  if (it == s->attached.end()) return fail(TOS_ERR_INVALID_ARG, "catalogue is not attached");
+  if (s->pending.count(cat)) return fail(TOS_ERR_INVALID_ARG, "catalogue has unfinished requests");
+  s->adm.remove_resident(it->second);
+  s->attached.erase(it);
+  s->dispatch();
+  return TOS_OK;
+}
+
+tos_status tos_server_submit(tos_server* s, tos_catalog* cat, const tos_grid* grid, double scale,
+                             uint32_t flags, uint64_t* request_id) {
+  if (!s || !cat || !grid || !request_id) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  double max_ang = 0;
+  TOS_TRY(tos_grid_max_angular_scale(grid, scale, &max_ang));
+  if (flags & ~(TOS_XI_SUBSAMPLES | TOS_XI_EXACT | TOS_XI_PER_GROUP))
+    return fail(TOS_ERR_INVALID_ARG, "unknown flags");
+  if ((flags & TOS_XI_SUBSAMPLES) && (flags & TOS_XI_PER_GROUP))
+    return fail(TOS_ERR_INVALID_ARG, "TOS_XI_PER_GROUP and TOS_XI_SUBSAMPLES are exclusive");
+  std::unique_ptr<Request> r(new Request());
+  r->cat = cat;
+  r->grid = *grid;
+  r->scale = scale;
+  r->flags = flags;
+  r->n_rows = (flags & TOS_XI_SUBSAMPLES) ? cat->cells.size()
+              : (flags & TOS_XI_PER_GROUP) ? cat->groups.size()
+                                           : 0;
+  r->need = workspace_estimate(cat, *grid, scale, r->n_rows);
+  r->info.workspace_bytes = r->need;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) return fail(TOS_ERR_INVALID_ARG, "server is shutting down");
+  if (!s->attached.count(cat)) return fail(TOS_ERR_INVALID_ARG, "catalogue is not attached");
+  if (!s->adm.can_ever_fit(r->need))
+    return fail(TOS_ERR_OOM, "request needs about " + std::to_string(r->need) +
+                                 " bytes of workspace: more than the budget leaves beside the "
+                                 "resident catalogues");
+  r->id = s->next_id++;
+  r->info.submit_s = s->now();
+  r->info.slot = -1;
+  *request_id = r->id;
+  s->pending[cat]++;
+  s->queue.push_back(r.get());
+  s->reqs[r->id] = std::move(r);
+  s->dispatch();
+  return TOS_OK;
+}
+
+tos_status tos_server_wait(tos_server* s, uint64_t id, tos_xibin* out_bins, tos_xibin* out_rows,
+                           tos_xi_stats* stats, tos_request_info* info) {
+  if (!s) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  std::unique_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return fail(TOS_ERR_INVALID_ARG, "unknown request id");
+    Request* p = it->second.get();
+    s->cv_done.wait(lk, [&] { return p->done; });
+    r = std::move(it->second);
+    s->reqs.erase(it);
+  }
+  if (info) *info = r->info;
+  if (r->status != TOS_OK) return fail(r->status, r->error);
+  if (out_bins) std::copy(r->bins.begin(), r->bins.end(), out_bins);
+  if (out_rows && r->n_rows) std::copy(r->rows.begin(), r->rows.end(), out_rows);
+  if (stats) *stats = r->stats;
+  return TOS_OK;
+}
+
+tos_status tos_server_status_get(tos_server* s, tos_server_status* out) {
+  if (!s || !out) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  out->budget_bytes = s->adm.budget();
+  out->resident_bytes = s->adm.resident();
+  out->in_use_bytes = s->adm.in_use();
+  out->peak_bytes = s->peak;
+  out->queued = s->queue.size();
+  uint64_t running = 0;
+  for (auto* r : s->assigned) running += (r != nullptr);
+  out->running = running;
+  out->completed = s->completed;
+  out->slots = (uint32_t)s->engines.size();
+  return TOS_OK;
+}
+
+}  // extern "C"

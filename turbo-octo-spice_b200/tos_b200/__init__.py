@@ -59,6 +59,23 @@ class XiStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class RequestInfo(C.Structure):
+    _fields_ = [("submit_s", C.c_double), ("start_s", C.c_double), ("end_s", C.c_double),
+                ("slot", C.c_int32), ("reserved", C.c_int32), ("workspace_bytes", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+class ServerStatus(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("budget_bytes", "resident_bytes", "in_use_bytes", "peak_bytes",
+                                           "queued", "running", "completed")] + [
+        ("slots", C.c_uint32), ("reserved", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
 _lib = None
 
 
@@ -70,6 +87,7 @@ def lib() -> C.CDLL:
             raise RuntimeError(f"engine library not built: {LIB_PATH} (run make in {PKG_ROOT})")
         L = C.CDLL(LIB_PATH)
         vp, sz, i32, u32, dbl = C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_double
+        u64 = C.c_uint64
         L.tos_last_error.restype = C.c_char_p
         L.tos_abi_version.restype = C.c_int
         L.tos_engine_create.argtypes = [i32, C.POINTER(vp)]
@@ -95,6 +113,15 @@ def lib() -> C.CDLL:
         L.tos_xi_jackknife.argtypes = [vp, vp, i32, sz, C.POINTER(sz), vp, vp, vp]
         L.tos_xi_run_jackknife.argtypes = [vp, vp, C.POINTER(_Grid), dbl, u32, i32, sz, C.POINTER(sz),
                                            vp, vp, vp, vp, C.POINTER(XiStats)]
+        L.tos_server_create.argtypes = [i32, i32, u64, C.POINTER(vp)]
+        L.tos_server_destroy.argtypes = [vp]
+        L.tos_server_destroy.restype = None
+        L.tos_server_attach.argtypes = [vp, vp]
+        L.tos_server_detach.argtypes = [vp, vp]
+        L.tos_server_submit.argtypes = [vp, vp, C.POINTER(_Grid), dbl, u32, C.POINTER(u64)]
+        L.tos_server_wait.argtypes = [vp, u64, vp, vp, C.POINTER(XiStats), C.POINTER(RequestInfo)]
+        L.tos_server_status_get.argtypes = [vp, C.POINTER(ServerStatus)]
+        L.tos_catalog_device_bytes.argtypes = [vp, C.POINTER(u64)]
         L.tos_comoving_distance.argtypes = [dbl, vp, sz, vp]
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
         for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
@@ -236,6 +263,11 @@ class Catalog:
         _check(lib().tos_catalog_sightline_cells(self._h, _ptr(out), self.n_sightlines))
         return out
 
+    def device_bytes(self) -> int:
+        n = C.c_uint64()
+        _check(lib().tos_catalog_device_bytes(self._h, C.byref(n)))
+        return n.value
+
     def num_groups(self) -> int:
         n = C.c_size_t()
         _check(lib().tos_catalog_num_groups(self._h, C.byref(n)))
@@ -302,6 +334,69 @@ def xi_run_jackknife(engine: Engine, catalog: Catalog, grid: Grid, scale: float,
     _check(L.tos_xi_run_jackknife(engine.handle, catalog.handle, C.byref(g), scale, flags, region_order, nk,
                                   C.byref(n), _ptr(ids), _ptr(bins), _ptr(groups), _ptr(drop), C.byref(st)))
     return ids, bins, groups, drop, st.as_dict()
+
+
+class Server:
+    """Request server over resident catalogues (tos_server): worker slots with
+    their own streams, admission in arrival order under a device-memory budget."""
+
+    def __init__(self, device: int = 0, slots: int = 4, memory_budget_bytes: int = 150 * 10**9):
+        h = C.c_void_p()
+        _check(lib().tos_server_create(device, slots, memory_budget_bytes, C.byref(h)))
+        self._h = h
+
+    def attach(self, catalog: Catalog):
+        _check(lib().tos_server_attach(self._h, catalog.handle))
+
+    def detach(self, catalog: Catalog):
+        _check(lib().tos_server_detach(self._h, catalog.handle))
+
+    def submit(self, catalog: Catalog, grid: Grid, scale: float, subsamples: bool = False,
+               per_group: bool = False, exact: bool = False) -> "ServerRequest":
+        flags = ((XI_SUBSAMPLES if subsamples else 0) | (XI_EXACT if exact else 0) |
+                 (XI_PER_GROUP if per_group else 0))
+        rid = C.c_uint64()
+        _check(lib().tos_server_submit(self._h, catalog.handle, C.byref(grid.c_struct()), scale, flags,
+                                       C.byref(rid)))
+        rows = catalog.num_cells() if subsamples else catalog.num_groups() if per_group else 0
+        return ServerRequest(self, rid.value, grid.nbins, rows)
+
+    def status(self) -> dict:
+        st = ServerStatus()
+        _check(lib().tos_server_status_get(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tos_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class ServerRequest:
+    """A submitted request; wait() blocks and returns (bins, rows or None, stats, info)."""
+
+    def __init__(self, server: Server, rid: int, nbins: int, n_rows: int):
+        self.server, self.id, self.nbins, self.n_rows = server, rid, nbins, n_rows
+
+    def wait(self):
+        bins = np.zeros(self.nbins, dtype=XIBIN_DTYPE)
+        rows = np.zeros((self.n_rows, self.nbins), dtype=XIBIN_DTYPE) if self.n_rows else None
+        st, info = XiStats(), RequestInfo()
+        _check(lib().tos_server_wait(self.server._h, self.id, _ptr(bins),
+                                     _ptr(rows) if rows is not None else None, C.byref(st), C.byref(info)))
+        return bins, rows, st.as_dict(), info.as_dict()
 
 
 def finalize(bins: np.ndarray) -> np.ndarray:
