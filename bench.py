@@ -10,7 +10,12 @@ counted as the reference counts them (sum of N_i*N_j over accepted sightline
 pairs, XiEstimator.cc:149).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                  [--workload full|small|brute]
+                  [--workload full|small|brute] [--mocks M] [--requests R]
+
+With one GPU the line also carries "batched" (plain vs batched pixel-pairs/s
+on the first M mocks of the batched configuration, and the one-pass
+jackknife) and "serving" (p50/p99 latency and pixel-pairs/s of a Poisson
+request stream with several slots and with one).
 
 N>1: launched by torchrun, one rank per GPU; every rank processes the whole
 catalogue (independent replicas, weak scaling); times are the max over ranks.
@@ -55,11 +60,17 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--workload", choices=["full", "small", "brute"], default="full")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=18.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sightlines", type=int, default=160000,
                     help="full workload: sightlines over the same ~10000 deg^2 (profiling uses fewer)")
+    ap.add_argument("--mocks", type=int, default=2,
+                    help="batched sample: the first M mocks of the seeded 256-mock draw (0: skip)")
+    ap.add_argument("--requests", type=int, default=12,
+                    help="serving sample: Poisson requests at 20/s over a resident pool (0: skip)")
+    ap.add_argument("--serve-max", type=int, default=20000,
+                    help="serving sample: largest pool catalogue (sightlines), bounding the bench's time")
     return ap.parse_args()
 
 
@@ -373,6 +384,15 @@ def engine_arm(args, D):
         line["grid_sweep_sightline_pairs_per_step"] = int(st["num_grid_items"])
         line["run_sweep_sightline_pairs_per_step"] = int(st["num_run_items"])
         line["ms_expand"] = st["ms_expand"]
+    if D.rank == 0 and D.world == 1 and "pts" not in W:
+        if args.mocks > 0:
+            t = time.perf_counter()
+            line["batched"] = batched_measure(eng, args.mocks, 1)
+            line["batched"]["section_wall_s"] = time.perf_counter() - t
+        if args.requests > 0:
+            t = time.perf_counter()
+            line["serving"] = serving_measure(W, args.requests, args.serve_max)
+            line["serving"]["section_wall_s"] = time.perf_counter() - t
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
         v, desc = cpu_sample(W, args.cpu_seconds, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
@@ -380,6 +400,157 @@ def engine_arm(args, D):
     if D.rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
+
+
+# ---------------------------------------------------------------- batched and served
+def reduced(los, px, keep):
+    """The sightlines where keep is true, with their pixels in a compact layout."""
+    r_los = los[keep].copy()
+    chunks, off = [], 0
+    for s in range(len(r_los)):
+        o, n = int(r_los[s]["pixel_offset"]), int(r_los[s]["num_pixels"])
+        chunks.append(px[o:o + n])
+        r_los[s]["pixel_offset"] = off
+        off += n
+    return r_los, np.concatenate(chunks)
+
+
+def batched_measure(eng, n_mocks, reps):
+    """Plain vs batched on a bounded sample of the batched configuration: the
+    first M mocks of the seeded 256-mock draw (sightline counts log-uniform in
+    [2k, 40k], each on its own cap at 16 per deg^2), (r, mu) 50x20 bins to
+    200 Mpc/h.  plain = one catalogue and one pair count per mock, one after
+    another; batched = one catalogue holding every mock as a sightline group
+    and one TOS_XI_PER_GROUP count.  Both wall-clock, catalogues resident.
+    Jackknife: every (mock, HEALPix nside=8 region) subsample in one pass,
+    against separate runs on reduced catalogues (a few timed, scaled to all)."""
+    import tos_b200 as T
+    from tos_b200 import synth
+    parts, scale = synth.mock_batch(n_mocks=n_mocks, seed=11)
+    g = T.Grid.polar("[0:200]*50", "[0:1]*20")
+    los, px = synth.merge_groups(parts)
+    bcat = T.Catalog(eng, los, px, 6)
+    cats = [T.Catalog(eng, l, p, 6) for l, p in parts]
+    T.xi_run(eng, bcat, g, scale, per_group=True)  # warm-up
+    for c in cats:
+        T.xi_run(eng, c, g, scale)
+    t_b, t_p = [], []
+    for _ in range(reps):
+        t = time.perf_counter()
+        _, rows, bst = T.xi_run(eng, bcat, g, scale, per_group=True)
+        t_b.append(time.perf_counter() - t)
+    for _ in range(reps):
+        t = time.perf_counter()
+        got = [T.xi_run(eng, c, g, scale) for c in cats]
+        t_p.append(time.perf_counter() - t)
+    for k, x in enumerate(got):  # the same pairs, mock by mock
+        assert np.array_equal(rows[k]["num_pairs"], x[0]["num_pairs"])
+    pairs = int(bst["num_pixel_pairs"])
+    assert pairs == sum(int(x[2]["num_pixel_pairs"]) for x in got)
+    tb, tp = float(np.median(t_b)), float(np.median(t_p))
+    # jackknife subsamples: one pass against a few separate runs
+    t = time.perf_counter()
+    ids, _, _, drop, _ = T.xi_run_jackknife(eng, bcat, g, scale, 3)
+    t_jk = time.perf_counter() - t
+    reg = synth.ang2pix_ring(8, 0.5 * math.pi - los["dec"], los["ra"])
+    times = []
+    for key in ids[:: max(1, len(ids) // 3)][:3]:
+        gid, rid = int(key) >> 32, int(key) & 0xFFFFFFFF
+        mine = los["group"] == gid
+        r_los, r_px = reduced(parts[gid][0], parts[gid][1], reg[mine] != rid)
+        rc = T.Catalog(eng, r_los, r_px, 6)
+        t = time.perf_counter()
+        rb, _, _ = T.xi_run(eng, rc, g, scale)
+        times.append(time.perf_counter() - t)
+        rc.close()
+        k = int(np.nonzero(ids == key)[0][0])
+        assert np.array_equal(rb["num_pairs"], drop[k]["num_pairs"])
+    bcat.close()
+    for c in cats:
+        c.close()
+    sep = float(np.mean(times))
+    return {"workload": f"first {len(parts)} mocks of the seeded 256-mock draw (counts log-uniform "
+                        "[2k,40k], own cap each at 16/deg^2), (r,mu) 50x20 bins to 200 Mpc/h, nside=64 cells",
+            "mocks": len(parts), "sightlines": int(len(los)), "pixels": int(len(px)), "pixel_pairs": pairs,
+            "plain": {"value": pairs / tp, "unit": UNIT, "wall_s": tp,
+                      "how": "one catalogue and one tos_xi_run per mock, in turn"},
+            "batched": {"value": pairs / tb, "unit": UNIT, "wall_s": tb, "device_ms": bst["ms_device"],
+                        "how": "one catalogue with a sightline group per mock, one TOS_XI_PER_GROUP run"},
+            "speedup": tp / tb, "reps": reps,
+            "jackknife": {"subsamples": int(len(ids)), "region": "HEALPix nside=8 within each mock",
+                          "one_pass_s": t_jk, "separate_run_s_mean": sep, "separate_runs_timed": len(times),
+                          "separate_all_s_estimated": sep * len(ids),
+                          "speedup_estimated": sep * len(ids) / t_jk}}
+
+
+def serving_measure(W, n_requests, serve_max, slots_list=(4, 1)):
+    """The serving pattern on a resident pool: 6 catalogues whose sightline
+    counts are drawn log-uniform in [1k, 160k] and capped at serve_max (the
+    first N sightlines of the full-survey catalogue, a uniform subsample of
+    it; a 160k request alone takes ~19 s, so the cap bounds the bench's
+    time), requests arriving as a
+    Poisson stream at 20/s, each for a pool catalogue at random with
+    (r_par,r_perp) 50x50 or (r,mu) 50x20 binning at random, admitted under a
+    150 GB budget.  Run once with several slots (continuous admission) and
+    once with one slot (one request at a time)."""
+    import threading
+
+    import tos_b200 as T
+    rng = np.random.default_rng(2024)
+    counts = np.sort(np.exp(rng.uniform(math.log(1000), math.log(160000), 6)).astype(int))
+    counts = np.minimum(counts, min(serve_max, len(W["los"])))
+    arrivals = np.cumsum(rng.exponential(1 / 20.0, n_requests))
+    picks = rng.integers(0, len(counts), n_requests)
+    grids = [T.Grid.cartesian(), T.Grid.polar("[0:200]*50", "[0:1]*20")]
+    gpick = rng.integers(0, 2, n_requests)
+    los, px = W["los"], W["px"]
+    out = {"workload": "pool of 6 resident catalogues (first N sightlines of the full survey, N log-uniform "
+                       f"[1k,160k] capped at {serve_max}), Poisson arrivals at 20/s, binning (r_par,r_perp) "
+                       "50x50 or (r,mu) 50x20 at random, 150 GB budget, FIFO admission",
+           "pool_sightlines": [int(c) for c in counts], "requests": int(n_requests)}
+    for slots in slots_list:
+        srv = T.Server(0, slots=slots, memory_budget_bytes=150 * 10**9)
+        eng = T.Engine(0)
+        pool = []
+        for n in counts:
+            end = int(los[n - 1]["pixel_offset"] + los[n - 1]["num_pixels"])
+            c = T.Catalog(eng, los[:n], px[:end], W["order"])
+            srv.attach(c)
+            pool.append(c)
+        for c in pool[:2]:  # warm-up
+            for g in grids:
+                srv.submit(c, g, W["scale"]).wait()
+        reqs = [None] * n_requests
+
+        def feeder():
+            t0 = time.perf_counter()
+            for k in range(n_requests):
+                d = arrivals[k] - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                reqs[k] = srv.submit(pool[picks[k]], grids[gpick[k]], W["scale"])
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        th.join()
+        lat, pairs, first, last = [], 0, None, None
+        for r in reqs:
+            _, _, st, info = r.wait()
+            lat.append(info["end_s"] - info["submit_s"])
+            pairs += int(st["num_pixel_pairs"])
+            first = info["submit_s"] if first is None else min(first, info["submit_s"])
+            last = info["end_s"] if last is None else max(last, info["end_s"])
+        status = srv.status()
+        srv.close()
+        for c in pool:
+            c.close()
+        eng.close()
+        span = last - first
+        out[f"slots_{slots}"] = {"value": pairs / span, "unit": UNIT, "makespan_s": span,
+                                 "p50_latency_s": float(np.percentile(lat, 50)),
+                                 "p99_latency_s": float(np.percentile(lat, 99)),
+                                 "pixel_pairs": pairs, "peak_device_bytes": int(status["peak_bytes"])}
+    return out
 
 
 def main():
