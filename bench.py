@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sightlines", type=int, default=160000,
                     help="full workload: sightlines over the same ~10000 deg^2 (profiling uses fewer)")
+    ap.add_argument("--grid", choices=["cartesian", "polar"], default="cartesian",
+                    help="binning of the plain workloads: (r_par,r_perp) 50x50 or (r,mu) 50x20")
     ap.add_argument("--mocks", type=int, default=2,
                     help="batched sample: the first M mocks of the seeded 256-mock draw (0: skip)")
     ap.add_argument("--requests", type=int, default=12,
@@ -168,25 +170,31 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- workloads
-def make_workload(kind, n_full=160000):
+def make_workload(kind, n_full=160000, binning="cartesian"):
     from tos_b200 import Grid, synth
+    if binning == "polar":
+        grid, gdesc, gspec = (Grid.polar("[0:200]*50", "[0:1]*20"), "(r,mu) 50x20 bins to 200 Mpc/h",
+                              "polar [0:200]*50 [0:1]*20 [3.556:3.735]*1")
+    else:
+        grid, gdesc, gspec = (Grid.cartesian(), "(r_par,r_perp) 50x50 bins to 200 Mpc/h",
+                              "cartesian [0:200]*50 [0:200]*50 [3.556:3.735]*1")
+    suffix = "" if binning == "cartesian" else "_" + binning
     if kind == "full":
         los, px, meta = synth.full_survey(n_full, seed=7)
-        name = "plain_full_survey" if n_full == 160000 else f"plain_full_survey_{n_full}"
-        return dict(name=name, los=los, px=px, scale=meta["scale"], grid=Grid.cartesian(),
-                    order=6, ops="cartesian",
+        name = ("plain_full_survey" if n_full == 160000 else f"plain_full_survey_{n_full}") + suffix
+        return dict(name=name, los=los, px=px, scale=meta["scale"], grid=grid,
+                    order=6, ops=binning,
                     config={"workload": f"plain method, full survey: {n_full} sightlines, ~10000 deg^2, "
-                                        "(r_par,r_perp) 50x50 bins to 200 Mpc/h, HEALPix nside=64",
+                                        f"{gdesc}, HEALPix nside=64",
                             "sightlines": n_full, "pixels": int(meta["num_pixels"]),
                             "pixels_per_sightline_min_mean_max": meta["pixels_per_sightline"],
-                            "grid": "cartesian [0:200]*50 [0:200]*50 [3.556:3.735]*1", "healpix_order": 6,
-                            "seed": 7})
+                            "grid": gspec, "healpix_order": 6, "seed": 7})
     if kind == "small":
         los, px, meta = synth.small_patch(2000, seed=1)
-        return dict(name="plain_small", los=los, px=px, scale=meta["scale"], grid=Grid.cartesian(), order=6,
-                    ops="cartesian",
-                    config={"workload": "plain method, small: 2000 sightlines on a 10x10 deg patch, "
-                                        "(r_par,r_perp) 50x50 bins, HEALPix nside=64",
+        return dict(name="plain_small" + suffix, los=los, px=px, scale=meta["scale"], grid=grid, order=6,
+                    ops=binning,
+                    config={"workload": f"plain method, small: 2000 sightlines on a 10x10 deg patch, "
+                                        f"{gdesc}, HEALPix nside=64",
                             "sightlines": 2000, "pixels": int(meta["num_pixels"]), "seed": 1})
     pts = synth.grf_grid(64, 256.0, seed=3)
     return dict(name="brute_grf64", pts=pts, ops="brute",
@@ -239,7 +247,7 @@ def cpu_sample(W, seconds, nthreads):
 def reference_arm(args, D):
     if D.rank != 0:
         return
-    W = make_workload(args.workload, args.sightlines)
+    W = make_workload(args.workload, args.sightlines, args.grid)
     nthreads = os.cpu_count() or 1
     per_step = max(5.0, min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
@@ -280,7 +288,7 @@ def load_traffic(name):
 def engine_arm(args, D):
     import torch
     import tos_b200 as T
-    W = make_workload(args.workload, args.sightlines)
+    W = make_workload(args.workload, args.sightlines, args.grid)
     dev = D.local
     eng = T.Engine(dev)
     ops = OPS_PER_PAIR[W["ops"]]
@@ -334,7 +342,8 @@ def engine_arm(args, D):
         grid_frac = st["num_grid_items"] / max(1, st["num_sightline_pairs_used"])
         by_grid = grid_frac >= 0.99
         kernel_ms = (ms_grid if by_grid else ms_pairs) / args.steps
-        kernel_name = "grid_kernel" if by_grid else "grid/run/pair kernels"
+        kernel_name = ("grid_kernel" if by_grid else
+                       "pair_kernel" if st["num_run_items"] == 0 else "grid/run/pair kernels")
         evaluated = int(st["num_pixel_pairs_evaluated"])
         launches = LAUNCHES_PER_RUN * args.steps
         cat.close()

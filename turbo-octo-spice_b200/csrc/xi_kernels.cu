@@ -76,6 +76,25 @@ __device__ void add_direct(const PairArgs& A, uint32_t cell, uint32_t idx, const
   atomicAdd(&A.counters[3], 1ull);
 }
 
+// Add field k's split fixed-point words (sums over at most a window slot's
+// contributions) to the 128-bit global sum at base: signed fields carry
+// lo + mid * 2^22 + hi * 2^44 (hi signed), positive fields lo + hi * 2^22.
+__device__ __forceinline__ void add_words(unsigned long long* base, int k, uint32_t lo,
+                                          uint32_t mid, uint32_t hi_bits) {
+  if (k < kSigned) {
+    const int hi = (int)hi_bits;
+    const unsigned long long l0 = (unsigned long long)lo + ((unsigned long long)mid << kSplit);
+    const unsigned long long l1 = l0 + ((unsigned long long)(hi & 0xFFFFF) << 44);
+    const long long h = (long long)(hi >> 20) + (l1 < l0 ? 1 : 0);
+    const unsigned long long old = atomicAdd(base + k, l1);
+    const long long hh = h + ((old + l1 < old) ? 1 : 0);
+    if (hh != 0) atomicAdd(base + 7 + k, (unsigned long long)hh);
+  } else {
+    const int hi = (int)mid;
+    add128(base + k, base + 7 + k, ((long long)hi << kSplit) + (long long)lo);
+  }
+}
+
 // Move the warp window into the global accumulators and clear it.
 template <int COORD>
 __device__ void flush_window(const PairArgs& A, const Item& it, uint32_t* win, int lane) {
@@ -99,23 +118,9 @@ __device__ void flush_window(const PairArgs& A, const Item& it, uint32_t* win, i
     if (idx < A.g.ntotal) {
       unsigned long long* base = acc_base(A, it.cell, idx);
 #pragma unroll
-      for (int k = 0; k < 7; ++k) {
-        const uint32_t lo = win[wword(k, 0) * S + s];
-        if (k < kSigned) {
-          // value = hi * 2^44 + mid * 2^22 + lo as a 128-bit number
-          const uint32_t mid = win[wword(k, 1) * S + s];
-          const int hi = (int)win[wword(k, 2) * S + s];
-          const unsigned long long l0 = (unsigned long long)lo + ((unsigned long long)mid << kSplit);
-          const unsigned long long l1 = l0 + ((unsigned long long)(hi & 0xFFFFF) << 44);
-          const long long h = (long long)(hi >> 20) + (l1 < l0 ? 1 : 0);
-          const unsigned long long old = atomicAdd(base + k, l1);
-          const long long hh = h + ((old + l1 < old) ? 1 : 0);
-          if (hh != 0) atomicAdd(base + 7 + k, (unsigned long long)hh);
-        } else {
-          const int hi = (int)win[wword(k, 1) * S + s];
-          add128(base + k, base + 7 + k, ((long long)hi << kSplit) + (long long)lo);
-        }
-      }
+      for (int k = 0; k < 7; ++k)
+        add_words(base, k, win[wword(k, 0) * S + s], win[wword(k, 1) * S + s],
+                  k < kSigned ? win[wword(k, 2) * S + s] : 0u);
       atomicAdd(base + 14, (unsigned long long)cnt);
     } else {
       atomicAdd(&A.counters[2], (unsigned long long)cnt);
@@ -222,23 +227,22 @@ __device__ __forceinline__ void make_contrib(const Row& R, uint32_t m, double dw
   o.c[6] = __fma_rn(R.hl1, md, 0.5 * dl);
 }
 
-// Add the runs closed by lanes with `emit` into the warp window: lanes that
-// close a run in the same slot are summed with redux.sync and one of them adds
-// the sums.  Keys outside the window go straight to the global accumulators.
+// Add the runs closed by lanes with `emit`: lanes that close a run with the
+// same key are summed with redux.sync on the split fixed-point words and one
+// of them adds the sums, to the warp window, or straight to the global
+// accumulators for keys outside the window.  The fixed-point values are the
+// same either way, so the integer totals do not depend on the grouping.
 // Returns (warp-uniform) whether some slot reached its capacity.
 template <int COORD>
 __device__ __forceinline__ bool emit_runs(const PairArgs& A, const Item& it, uint32_t* win,
                                           int lane, bool emit, uint32_t key, const Contrib& ct) {
   int slot = -1;
-  if (emit) {
-    slot = window_slot<COORD>(A, it, key);
-    if (slot < 0) add_direct(A, it.cell, flat_index<COORD>(A, it, key), ct.c, ct.m);
-  }
-  unsigned pending = __ballot_sync(kFull, emit && slot >= 0);
+  if (emit) slot = window_slot<COORD>(A, it, key);
+  unsigned pending = __ballot_sync(kFull, emit);
   bool full = false;
   if (pending) {
     uint32_t wv[kWordCount];
-    if (emit && slot >= 0) {
+    if (emit) {
 #pragma unroll
       for (int k = 0; k < 7; ++k) {
         if (k < kSigned) {
@@ -256,21 +260,41 @@ __device__ __forceinline__ bool emit_runs(const PairArgs& A, const Item& it, uin
     const int S = A.win_slots;
     while (pending) {
       const int leader = __ffs(pending) - 1;
-      const int ls = __shfl_sync(kFull, slot, leader);
-      const unsigned peers = __ballot_sync(kFull, ((pending >> lane) & 1u) && slot == ls);
+      const uint32_t lkey = __shfl_sync(kFull, key, leader);
+      const unsigned peers = __ballot_sync(kFull, ((pending >> lane) & 1u) && key == lkey);
       if ((peers >> lane) & 1u) {
         const bool lead = lane == leader;
+        if (slot >= 0) {  // the same for every peer: the slot is a function of the key
 #pragma unroll
-        for (int w = 0; w < kWordCount; ++w) {
-          const uint32_t sw = __reduce_add_sync(peers, wv[w]);
-          if (lead) atomicAdd(&win[w * S + ls], sw);
-        }
-        const uint32_t sm = __reduce_add_sync(peers, ct.m);
-        if (lead) {
-          atomicAdd(&win[kWordCount * S + ls], sm);
-          const uint32_t n = (uint32_t)__popc(peers);
-          const uint32_t old = atomicAdd(&win[kWordContrib * S + ls], n);
-          full = old + n > kSlotCap;
+          for (int w = 0; w < kWordCount; ++w) {
+            const uint32_t sw = __reduce_add_sync(peers, wv[w]);
+            if (lead) atomicAdd(&win[w * S + slot], sw);
+          }
+          const uint32_t sm = __reduce_add_sync(peers, ct.m);
+          if (lead) {
+            atomicAdd(&win[kWordCount * S + slot], sm);
+            const uint32_t n = (uint32_t)__popc(peers);
+            const uint32_t old = atomicAdd(&win[kWordContrib * S + slot], n);
+            full = old + n > kSlotCap;
+          }
+        } else {
+          uint32_t sw[kWordCount];
+#pragma unroll
+          for (int w = 0; w < kWordCount; ++w) sw[w] = __reduce_add_sync(peers, wv[w]);
+          const uint32_t sm = __reduce_add_sync(peers, ct.m);
+          if (lead) {
+            const uint32_t idx = flat_index<COORD>(A, it, lkey);
+            if (idx < A.g.ntotal) {
+              unsigned long long* base = acc_base(A, it.cell, idx);
+#pragma unroll
+              for (int k = 0; k < 7; ++k)
+                add_words(base, k, sw[wword(k, 0)], sw[wword(k, 1)], k < kSigned ? sw[wword(k, 2)] : 0u);
+              atomicAdd(base + 14, (unsigned long long)sm);
+              atomicAdd(&A.counters[3], 1ull);
+            } else {
+              atomicAdd(&A.counters[2], (unsigned long long)sm);
+            }
+          }
         }
       }
       pending &= ~peers;
