@@ -15,6 +15,7 @@
 
 #include "engine_internal.h"
 #include "healpix.h"
+#include "fixed128.cuh"
 #include "xi_kernels.cuh"
 
 namespace tos {
@@ -250,19 +251,6 @@ __global__ void k_expand(const uint32_t* members, uint32_t n_members, const uint
 // Per bin: convert every cell's 128-bit fixed-point sums to double and add
 // them in ascending cell order (the order of xi_finalize_task,
 // XiEstimator.cc:298-305).
-// Signed 128-bit fixed-point value {lo, hi} as a double with one relative
-// rounding: the magnitude is converted, so a small negative value (hi = -1,
-// lo close to 2^64) loses no low bits to the rounding of lo.
-__device__ __forceinline__ double i128_to_double(unsigned long long lo, long long hi) {
-  const bool neg = hi < 0;
-  if (neg) {
-    lo = ~lo + 1ull;
-    hi = (long long)(~(unsigned long long)hi + (lo == 0ull ? 1ull : 0ull));
-  }
-  const double m = __fma_rn((double)hi, 18446744073709551616.0 /* 2^64 */, (double)lo);
-  return neg ? -m : m;
-}
-
 __global__ void k_combine(const unsigned long long* acc, uint32_t n_cells, uint32_t nb,
                           double4 inv_a, double4 inv_b, tos_xibin* out, tos_xibin* cells_out) {
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
@@ -277,7 +265,7 @@ __global__ void k_combine(const unsigned long long* acc, uint32_t n_cells, uint3
       double v[7];
 #pragma unroll
       for (int k = 0; k < 7; ++k) {
-        v[k] = (cnt != 0) ? i128_to_double(a[k], (long long)a[7 + k]) * inv[k] : 0.0;
+        v[k] = (cnt != 0) ? i128_double(acc128(a, k)) * inv[k] : 0.0;
         s[k] += v[k];
       }
       n += cnt;
@@ -324,7 +312,7 @@ __global__ void k_combine_groups(const unsigned long long* acc, const uint32_t* 
       const long long cnt = (long long)a[14];
       if (cnt == 0) continue;  // no pairs: zero sums (as k_combine)
 #pragma unroll
-      for (int k = 0; k < 7; ++k) s[k] += i128_to_double(a[k], (long long)a[7 + k]) * inv[k];
+      for (int k = 0; k < 7; ++k) s[k] += i128_double(acc128(a, k)) * inv[k];
       cnt_sum += cnt;
     }
     tos_xibin x;
@@ -1033,12 +1021,32 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
     TOS_CUDA_TRY(cub::DeviceReduce::Sum(ws->d_cub_tmp.p, tb, ws->d_cand.p, ctr + 5, nm, st));
     TOS_CUDA_TRY(cudaMemcpyAsync(&n_cand_total, ctr + 5, 8, cudaMemcpyDeviceToHost, st));
   }
+  std::vector<uint32_t> prim_items(nm);  // accepted pairs per primary sightline
+  TOS_CUDA_TRY(cudaMemcpyAsync(prim_items.data(), ws->d_cnt.p, (size_t)nm * 4,
+                               cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
   const uint64_t n_items = (uint64_t)last_off + last_cnt;
   unsigned long long n_pixel_pairs = 0, max_cell_pairs = 0;
   for (auto v : cell_pairs) {
     n_pixel_pairs += v;
     max_cell_pairs = std::max(max_cell_pairs, v);
+  }
+  {
+    // the carry-free accumulators take fewer than 2^32 adds per (row, bin):
+    // a sightline pair makes at most kMaxAddsPerItemBin * max_np of them
+    std::vector<uint64_t> cell_items(nc, 0);
+    for (uint32_t s = 0; s < nm; ++s) cell_items[cat->cell_idx[s]] += prim_items[s];
+    uint64_t max_row_items = 0;
+    if (plan)
+      max_row_items = plan->max_row_items(cell_items);
+    else
+      for (uint64_t v : cell_items) max_row_items = std::max(max_row_items, v);
+    const double adds = (double)max_row_items * kMaxAddsPerItemBin * std::max<double>(1, cat->max_np);
+    if (!(adds < 4294967296.0))
+      return fail(TOS_ERR_UNSUPPORTED,
+                  "up to " + std::to_string(max_row_items) +
+                      " sightline pairs share one accumulator row, which could pass 2^32 adds "
+                      "to one bin: use a finer HEALPix order");
   }
   // --- expansion pass 2: items
   TOS_TRY(ws->d_item_i.alloc(n_items));

@@ -168,6 +168,9 @@ struct RowPlan {
   std::function<tos_status(cudaStream_t, uint32_t nb, const double* inv_scale,
                            const unsigned long long* d_acc, tos_xibin* d_out)>
       combine;
+  // the most sightline pairs one row can receive, given the pairs whose
+  // primary lies in each cell
+  std::function<uint64_t(const std::vector<uint64_t>& cell_items)> max_row_items;
 };
 
 // The pair count behind tos_xi_run, with its scratch in `ws` (the caller

@@ -1,6 +1,7 @@
-// fixed128.cuh — reading the 128-bit fixed-point sums of the accumulator
-// rows ([row][bin][kAccWords]: field f's low word at f, high word at 7 + f,
-// the pair count at 14).
+// fixed128.cuh — reading the fixed-point sums of the accumulator rows
+// ([row][bin][kAccWords], the carry-free format described at kAccWords:
+// field f = hi * 2^32 + lo with lo at word f, hi at word 7 + f; the pair
+// count at word 14).
 #pragma once
 
 #include "xi_kernels.cuh"
@@ -9,7 +10,13 @@ namespace tos {
 
 // Field f of one (row, bin) as a signed 128-bit integer.
 __device__ __forceinline__ __int128 acc128(const unsigned long long* base, int f) {
-  return (__int128)(((unsigned __int128)(unsigned long long)base[7 + f] << 64) | base[f]);
+  return (__int128)(long long)base[7 + f] * (__int128)4294967296ll + (__int128)base[f];
+}
+
+// Store v (|v| < 2^95) as field f of a row kept in the same format.
+__device__ __forceinline__ void store128(unsigned long long* base, int f, __int128 v) {
+  base[f] = (unsigned long long)v & 0xFFFFFFFFull;
+  base[7 + f] = (unsigned long long)(long long)(v >> 32);
 }
 
 // Signed 128-bit value as a double with one relative rounding (by magnitude).

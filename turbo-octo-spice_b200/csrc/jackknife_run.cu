@@ -71,10 +71,7 @@ __global__ void k_group_totals(const unsigned long long* acc, uint32_t nb, const
     }
     unsigned long long* o = gtot + t * kAccWords;
 #pragma unroll
-    for (int f = 0; f < 7; ++f) {
-      o[f] = (unsigned long long)s[f];
-      o[7 + f] = (unsigned long long)(s[f] >> 64);
-    }
+    for (int f = 0; f < 7; ++f) store128(o, f, s[f]);
     o[14] = (unsigned long long)cnt;
     o[15] = 0;
     gout[t] = to_bin(s, cnt, inv);
@@ -257,6 +254,16 @@ extern "C" tos_status tos_xi_run_jackknife(tos_engine* e, tos_catalog* cat, cons
   plan.row_key = d_skey.p;
   plan.slot_start = d_slot_start.p;
   plan.slot_key = d_slot_key.p;
+  plan.max_row_items = [&](const std::vector<uint64_t>& cell_items) -> uint64_t {
+    // a pair of slot {a, b} has its primary in region a or b
+    std::vector<uint64_t> kitems(nk, 0);
+    for (size_t c = 0; c < nc; ++c) kitems[ckey[c]] += cell_items[c];
+    uint64_t m = 0;
+    for (uint32_t a = 0; a < nk; ++a)
+      for (uint32_t q = slot_start[a]; q < slot_start[a + 1]; ++q)
+        m = std::max(m, kitems[a] + (slot_key[q] != a ? kitems[slot_key[q]] : 0));
+    return m;
+  };
   plan.combine = [&](cudaStream_t st, uint32_t nb, const double* inv_scale,
                      const unsigned long long* d_acc, tos_xibin* d_out) -> tos_status {
     Inv7 inv;

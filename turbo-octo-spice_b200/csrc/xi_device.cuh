@@ -44,13 +44,15 @@ __device__ __forceinline__ int wword(int k, int p) {
 constexpr int kWordCount = 3 * kSigned + 2 * (7 - kSigned);      // 17
 constexpr int kWordContrib = kWordCount + 1;                     // 18
 
-// Add a signed 64-bit value to a 128-bit accumulator {lo: u64, hi: i64}.
-__device__ __forceinline__ void add128(unsigned long long* lo, unsigned long long* hi, long long q) {
-  const unsigned long long uq = (unsigned long long)q;
-  const unsigned long long old = atomicAdd(lo, uq);
-  const long long carry = (old + uq < old) ? 1 : 0;
-  const long long h = (q < 0 ? -1 : 0) + carry;
+// Add a signed value v (|v| < 2^95) to one field's sums {lo, hi} in the
+// carry-free format of kAccWords: lo += v mod 2^32, hi += floor(v / 2^32).
+__device__ __forceinline__ void add_wide(unsigned long long* lo, unsigned long long* hi, __int128 v) {
+  atomicAdd(lo, (unsigned long long)v & 0xFFFFFFFFull);
+  const long long h = (long long)(v >> 32);
   if (h != 0) atomicAdd(hi, (unsigned long long)h);
+}
+__device__ __forceinline__ void add128(unsigned long long* lo, unsigned long long* hi, long long q) {
+  add_wide(lo, hi, (__int128)q);
 }
 
 // ---- exact re-binning (reference expression order) returning the two axis

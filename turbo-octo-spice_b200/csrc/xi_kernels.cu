@@ -77,22 +77,17 @@ __device__ void add_direct(const PairArgs& A, uint32_t cell, uint32_t idx, const
 }
 
 // Add field k's split fixed-point words (sums over at most a window slot's
-// contributions) to the 128-bit global sum at base: signed fields carry
-// lo + mid * 2^22 + hi * 2^44 (hi signed), positive fields lo + hi * 2^22.
+// contributions) to the global sums at base: signed fields carry
+// lo + mid * 2^22 + hi * 2^44 (hi signed), positive fields lo + mid * 2^22.
 __device__ __forceinline__ void add_words(unsigned long long* base, int k, uint32_t lo,
                                           uint32_t mid, uint32_t hi_bits) {
-  if (k < kSigned) {
-    const int hi = (int)hi_bits;
-    const unsigned long long l0 = (unsigned long long)lo + ((unsigned long long)mid << kSplit);
-    const unsigned long long l1 = l0 + ((unsigned long long)(hi & 0xFFFFF) << 44);
-    const long long h = (long long)(hi >> 20) + (l1 < l0 ? 1 : 0);
-    const unsigned long long old = atomicAdd(base + k, l1);
-    const long long hh = h + ((old + l1 < old) ? 1 : 0);
-    if (hh != 0) atomicAdd(base + 7 + k, (unsigned long long)hh);
-  } else {
-    const int hi = (int)mid;
-    add128(base + k, base + 7 + k, ((long long)hi << kSplit) + (long long)lo);
-  }
+  __int128 v;
+  if (k < kSigned)
+    v = (__int128)(int)hi_bits * 17592186044416ll /* 2^44 */ + (__int128)((long long)mid << kSplit) +
+        (__int128)lo;
+  else
+    v = (__int128)(((long long)(int)mid << kSplit) + (long long)lo);
+  add_wide(base + k, base + 7 + k, v);
 }
 
 // Move the warp window into the global accumulators and clear it.

@@ -43,7 +43,17 @@ constexpr int kWinWords = 19;
 constexpr int kSplit = 22;      // bits in each low word of the fixed-point split
 constexpr int kSigned = 3;      // fields 0..2 are signed (3 words), 3..6 positive (2 words)
 constexpr uint32_t kSlotCap = 1024u - 64u;  // contributions per slot before the window is emptied
-constexpr int kAccWords = 16;   // u64 words per (cell, bin): 7 lo, 7 hi, count, unused
+// u64 words per (row, bin): field f's sum is hi[f] * 2^32 + lo[f], where
+// lo[f] (word f) is the unsigned sum of the low 32 bits of every value added
+// and hi[f] (word 7 + f) the signed sum of the values shifted right by 32.
+// The format carries nothing between words, so an add is two fire-and-forget
+// atomics; lo wraps after 2^32 adds to one (row, bin), which the host rules
+// out before a run (kMaxAddsPerItemBin).  Word 14: the pair count.
+constexpr int kAccWords = 16;
+// Adds one sightline pair can make to one (row, bin, field), per pixel of its
+// primary: at most two codes of a run-sweep lane per row and side, or three
+// runs of one key per row (monotone segments) plus window flushes.
+constexpr int kMaxAddsPerItemBin = 8;
 constexpr double kMagic52 = 6755399441055744.0;  // 1.5 * 2^52
 constexpr long long kMagic52Bits = 0x4338000000000000LL;
 
