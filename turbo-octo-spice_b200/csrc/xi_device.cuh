@@ -44,12 +44,18 @@ __device__ __forceinline__ int wword(int k, int p) {
 constexpr int kWordCount = 3 * kSigned + 2 * (7 - kSigned);      // 17
 constexpr int kWordContrib = kWordCount + 1;                     // 18
 
+// Global reduction add with no returned value (red, not atom): nothing in
+// the thread waits for it.
+__device__ __forceinline__ void red_add(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 // Add a signed value v (|v| < 2^95) to one field's sums {lo, hi} in the
 // carry-free format of kAccWords: lo += v mod 2^32, hi += floor(v / 2^32).
 __device__ __forceinline__ void add_wide(unsigned long long* lo, unsigned long long* hi, __int128 v) {
-  atomicAdd(lo, (unsigned long long)v & 0xFFFFFFFFull);
+  red_add(lo, (unsigned long long)v & 0xFFFFFFFFull);
   const long long h = (long long)(v >> 32);
-  if (h != 0) atomicAdd(hi, (unsigned long long)h);
+  if (h != 0) red_add(hi, (unsigned long long)h);
 }
 __device__ __forceinline__ void add128(unsigned long long* lo, unsigned long long* hi, long long q) {
   add_wide(lo, hi, (__int128)q);

@@ -72,7 +72,7 @@ __device__ void add_direct(const PairArgs& A, uint32_t cell, uint32_t idx, const
     add128(base + k, base + 7 + k,
            (k < kSigned || A.wide_all) ? to_fixed_wide(c[k], A.scale_hi[k])
                                        : to_fixed(c[k], A.scale[k]));
-  atomicAdd(base + 14, (unsigned long long)m);
+  red_add(base + 14, (unsigned long long)m);
   atomicAdd(&A.counters[3], 1ull);
 }
 
@@ -116,7 +116,7 @@ __device__ void flush_window(const PairArgs& A, const Item& it, uint32_t* win, i
       for (int k = 0; k < 7; ++k)
         add_words(base, k, win[wword(k, 0) * S + s], win[wword(k, 1) * S + s],
                   k < kSigned ? win[wword(k, 2) * S + s] : 0u);
-      atomicAdd(base + 14, (unsigned long long)cnt);
+      red_add(base + 14, (unsigned long long)cnt);
     } else {
       atomicAdd(&A.counters[2], (unsigned long long)cnt);
     }
@@ -284,7 +284,7 @@ __device__ __forceinline__ bool emit_runs(const PairArgs& A, const Item& it, uin
 #pragma unroll
               for (int k = 0; k < 7; ++k)
                 add_words(base, k, sw[wword(k, 0)], sw[wword(k, 1)], k < kSigned ? sw[wword(k, 2)] : 0u);
-              atomicAdd(base + 14, (unsigned long long)sm);
+              red_add(base + 14, (unsigned long long)sm);
               atomicAdd(&A.counters[3], 1ull);
             } else {
               atomicAdd(&A.counters[2], (unsigned long long)sm);

@@ -62,7 +62,7 @@ __device__ __forceinline__ void add_bin(const PairArgs& A, Dest d, int k, int c,
   unsigned long long* base = A.acc + ((size_t)d.cell * A.g.ntotal + idx) * kAccWords;
 #pragma unroll
   for (int f = 0; f < 7; ++f) add128(base + f, base + 7 + f, to_fixed_wide(F.s[f], A.scale_hi[f]));
-  atomicAdd(base + 14, (unsigned long long)F.n);
+  red_add(base + 14, (unsigned long long)F.n);
 }
 
 // Exact r_perp code of a pair: -1 below the axis, 0..n1-1, n1 above
