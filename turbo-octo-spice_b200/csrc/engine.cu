@@ -1164,6 +1164,8 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
       double R = rg.min0 + (double)n0 / rg.inv0;
       R = std::max(R, 0.0) * (1.0 + 1e-6) + 1e-6;
       const double dm = cat->max_d;
+      A.polar_r2 = R * R;
+      A.polar_e2 = std::ldexp(dm * dm, -23) + 1e-3;
       lim = (float)(std::sqrt(R * R + std::ldexp(dm * dm, -23) + 1e-3) * (1.0 + 1e-6) + 1e-3);
     } else {
       lim = first_axis_threshold(rg.min0, rg.inv0, n0, (int)n0);

@@ -53,16 +53,18 @@ __device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, 
   // boundaries loaded one row ahead
   const int r0 = min(r_lo + phase, r_hi - 1);
   ushort2 nQ = make_ushort2(qrow[(size_t)r0 * qstride], qrow[(size_t)r0 * qstride + 1]);
+  RowV nR = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, r0);
 #pragma unroll 1
   for (int r = r_lo + phase; r < r_hi; r += P) {
     const ushort2 Qv = nQ;
+    const RowV R = nR;
     const int rn = min(r + P, r_hi - 1);
     nQ = make_ushort2(qrow[(size_t)rn * qstride], qrow[(size_t)rn * qstride + 1]);
+    nR = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, rn);
     const int qa = min(max((int)Qv.x - fj, 0), nj), qb = min(max((int)Qv.y - fj, 0), nj);
     const int s = side ? qb : qa, e = side ? qa : qb;
     if (act && e > s) {
       n_eval += (unsigned long long)(e - s);
-      const RowV R = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, r);
       do_run<COORD, MINPOS>(A, d, colx, pre, c, R, k, s, e, acc, rech);
     }
   }

@@ -393,6 +393,20 @@ __device__ void process_item(const PairArgs& A, Item& it, uint32_t* win, int lan
   const double* rowwd = A.wd + oi;
   const float* roww = A.w + oi;
   const float4 rj = A.range[it.j];
+  // Column window |x1 - x2| < lim.  For Polar binning a pair is accepted only
+  // if r^2 = (d2 - d1)^2 + 2(1 - c) d1 d2 - err < R^2 (err: float rounding of
+  // d1^2, XiEstimator.cc:179-184), and d1 d2 >= dmin_i dmin_j when both
+  // sightlines' distances are positive, so the item's window narrows to
+  // |d2 - d1| < sqrt(R^2 - 2(1 - c) dmin_i dmin_j + err bound).
+  float lim = A.win_lim;
+  if (COORD == kPolar && A.prune) {
+    const float4 ri = A.range[it.i];
+    if (ri.x > 0.f && rj.x > 0.f) {
+      const double a = fmax(2.0 * (1.0 - it.c), 0.0);
+      const double q = A.polar_r2 - a * (double)ri.x * (double)rj.x * (1.0 - 1e-6) + A.polar_e2;
+      lim = fminf(lim, (float)(sqrt(fmax(q, 0.0)) * (1.0 + 1e-6) + 1e-3));
+    }
+  }
   for (uint32_t r0 = 0; r0 < it.ni; r0 += 32) {
     const uint32_t row = r0 + lane;
     const bool active = row < it.ni;
@@ -428,7 +442,7 @@ __device__ void process_item(const PairArgs& A, Item& it, uint32_t* win, int lan
     if (A.prune) {
       int lo = (int)it.nj, hi = 0;
       if (active) {
-        const float x1 = R.x1, lim = A.win_lim;
+        const float x1 = R.x1;
         lo = lower_bound_pred(it.colx, (int)it.nj, [&](float x2) { return __fsub_rn(x1, x2) < lim; });
         hi = lower_bound_pred(it.colx, (int)it.nj,
                               [&](float x2) { return x2 >= x1 && __fsub_rn(x2, x1) >= lim; });

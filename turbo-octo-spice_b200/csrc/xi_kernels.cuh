@@ -91,6 +91,8 @@ struct PairArgs {
   int bits0, bits1;          // bit patterns of mag0/mag1
   float r2_small;            // Polar: squared separations below this are re-binned in FP64
   float win_lim;             // |x1 - x2| >= win_lim (float) is always rejected
+  double polar_r2;           // Polar: R^2 of the largest accepted r (with margin), or 0
+  double polar_e2;           // Polar: bound on the float rounding of d1^2, plus margin
   int prune;                 // sightlines sorted: restrict columns to the r_par window
   // accumulation
   double scale[7];           // 2^F per field
