@@ -12,10 +12,12 @@ pairs, XiEstimator.cc:149).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
                   [--workload full|small|brute] [--mocks M] [--requests R]
 
-With one GPU the line also carries "batched" (plain vs batched pixel-pairs/s
-on the first M mocks of the batched configuration, and the one-pass
-jackknife) and "serving" (p50/p99 latency and pixel-pairs/s of a Poisson
-request stream with several slots and with one).
+With one GPU the line also carries "jackknife" (every nside=8
+delete-one-region subsample of the main catalogue in one pass, against one
+run per subsample), "batched" (plain vs batched pixel-pairs/s on the first M
+mocks of the batched configuration, and their one-pass jackknife) and
+"serving" (p50/p99 latency and pixel-pairs/s of a Poisson request stream
+with several slots and with one).
 
 N>1: launched by torchrun, one rank per GPU; every rank processes the whole
 catalogue (independent replicas, weak scaling); times are the max over ranks.
@@ -69,6 +71,8 @@ def parse():
                     help="binning of the plain workloads: (r_par,r_perp) 50x50 or (r,mu) 50x20")
     ap.add_argument("--mocks", type=int, default=2,
                     help="batched sample: the first M mocks of the seeded 256-mock draw (0: skip)")
+    ap.add_argument("--no-jackknife", action="store_true",
+                    help="skip the one-pass jackknife of the full-survey catalogue")
     ap.add_argument("--requests", type=int, default=12,
                     help="serving sample: Poisson requests at 20/s over a resident pool (0: skip)")
     ap.add_argument("--serve-max", type=int, default=20000,
@@ -346,6 +350,9 @@ def engine_arm(args, D):
                        "pair_kernel" if st["num_run_items"] == 0 else "grid/run/pair kernels")
         evaluated = int(st["num_pixel_pairs_evaluated"])
         launches = LAUNCHES_PER_RUN * args.steps
+        jk = None
+        if D.rank == 0 and D.world == 1 and not args.no_jackknife:
+            jk = jackknife_measure(eng, cat, W, ms_max / args.steps / 1e3, bins)
         cat.close()
         # end to end through the public API from pinned host buffers
         _tl, los_p = pinned_copy(W["los"])
@@ -394,6 +401,8 @@ def engine_arm(args, D):
         line["run_sweep_sightline_pairs_per_step"] = int(st["num_run_items"])
         line["ms_expand"] = st["ms_expand"]
     if D.rank == 0 and D.world == 1 and "pts" not in W:
+        if jk is not None:
+            line["jackknife"] = jk
         if args.mocks > 0:
             t = time.perf_counter()
             line["batched"] = batched_measure(eng, args.mocks, 1)
@@ -490,6 +499,42 @@ def batched_measure(eng, n_mocks, reps):
                           "one_pass_s": t_jk, "separate_run_s_mean": sep, "separate_runs_timed": len(times),
                           "separate_all_s_estimated": sep * len(ids),
                           "speedup_estimated": sep * len(ids) / t_jk}}
+
+
+def jackknife_measure(eng, cat, W, plain_step_s, plain_bins):
+    """Every delete-one-region subsample (HEALPix nside=8 regions) of the
+    workload's catalogue in one pass, against running the pair count once per
+    subsample on the reduced catalogue (one such run timed; all estimated from
+    it).  Delivered pairs are the binned pixel pairs of every subsample's
+    result, the unit both ways."""
+    import tos_b200 as T
+    from tos_b200 import synth
+    los, px, g = W["los"], W["px"], W["grid"]
+    t = time.perf_counter()
+    ids, bins, _, drop, st = T.xi_run_jackknife(eng, cat, g, W["scale"], 3)
+    t_one = time.perf_counter() - t
+    assert np.array_equal(bins["num_pairs"], plain_bins["num_pairs"])
+    reg = synth.ang2pix_ring(8, 0.5 * math.pi - los["dec"], los["ra"])
+    k = len(ids) // 2
+    r_los, r_px = reduced(los, px, reg != (int(ids[k]) & 0xFFFFFFFF))
+    rc = T.Catalog(eng, r_los, r_px, W["order"])
+    t = time.perf_counter()
+    rb, _, _ = T.xi_run(eng, rc, g, W["scale"])
+    t_sep = time.perf_counter() - t
+    rc.close()
+    assert np.array_equal(rb["num_pairs"], drop[k]["num_pairs"])
+    delivered = float(drop["num_pairs"].sum())
+    plain_rate = float(plain_bins["num_pairs"].sum()) / plain_step_s
+    return {"workload": "every delete-one-region subsample of the main catalogue, regions HEALPix nside=8",
+            "subsamples": int(len(ids)), "one_pass_s": t_one, "one_pass_device_ms": st["ms_device"],
+            "separate_run_s": t_sep, "separate_runs_timed": 1,
+            "separate_all_s_estimated": t_sep * len(ids),
+            "speedup_estimated": t_sep * len(ids) / t_one,
+            "unit": "binned pixel pairs/s",
+            "batched_value": delivered / t_one,
+            "plain_value": plain_rate,
+            "how": "batched: one tos_xi_run_jackknife pass; plain: one tos_xi_run per subsample "
+                   "on the catalogue without that region's sightlines"}
 
 
 def serving_measure(W, n_requests, serve_max, slots_list=(4, 1)):
