@@ -294,6 +294,9 @@ tos_status tos_server_submit(tos_server* server, tos_catalog* catalog, const tos
  * its flags ask for (NULL to drop them), stats and info optional. */
 tos_status tos_server_wait(tos_server* server, uint64_t request_id, tos_xibin* out_bins,
                            tos_xibin* out_rows, tos_xi_stats* stats, tos_request_info* info);
+/* Non-blocking: *done = 1 when the request has finished (tos_server_wait then
+ * returns at once), 0 while it is queued or running. */
+tos_status tos_server_poll(tos_server* server, uint64_t request_id, int* done);
 tos_status tos_server_status_get(tos_server* server, tos_server_status* out);
 
 /* Device bytes held by a catalogue (its data and the workspace of its own

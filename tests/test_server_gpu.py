@@ -137,5 +137,9 @@ def test_refusals(engine, catalogs):
         r = srv.submit(cat, GRIDS["polar"], scale)
         with pytest.raises(T.TosError):
             srv.detach(cat)  # a request is unfinished
+        while not r.done():  # poll without blocking
+            pass
         r.wait()
+        with pytest.raises(T.TosError):
+            r.done()  # the id is released by wait
         srv.detach(cat)

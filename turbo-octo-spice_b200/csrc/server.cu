@@ -312,6 +312,15 @@ tos_status tos_server_wait(tos_server* s, uint64_t id, tos_xibin* out_bins, tos_
   return TOS_OK;
 }
 
+tos_status tos_server_poll(tos_server* s, uint64_t id, int* done) {
+  if (!s || !done) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return fail(TOS_ERR_INVALID_ARG, "unknown request id");
+  *done = it->second->done ? 1 : 0;
+  return TOS_OK;
+}
+
 tos_status tos_server_status_get(tos_server* s, tos_server_status* out) {
   if (!s || !out) return fail(TOS_ERR_INVALID_ARG, "null argument");
   std::lock_guard<std::mutex> lk(s->mu);

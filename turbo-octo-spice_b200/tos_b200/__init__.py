@@ -121,6 +121,7 @@ def lib() -> C.CDLL:
         L.tos_server_submit.argtypes = [vp, vp, C.POINTER(_Grid), dbl, u32, C.POINTER(u64)]
         L.tos_server_wait.argtypes = [vp, u64, vp, vp, C.POINTER(XiStats), C.POINTER(RequestInfo)]
         L.tos_server_status_get.argtypes = [vp, C.POINTER(ServerStatus)]
+        L.tos_server_poll.argtypes = [vp, u64, C.POINTER(C.c_int)]
         L.tos_catalog_device_bytes.argtypes = [vp, C.POINTER(u64)]
         L.tos_comoving_distance.argtypes = [dbl, vp, sz, vp]
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
@@ -389,6 +390,12 @@ class ServerRequest:
 
     def __init__(self, server: Server, rid: int, nbins: int, n_rows: int):
         self.server, self.id, self.nbins, self.n_rows = server, rid, nbins, n_rows
+
+    def done(self) -> bool:
+        """Non-blocking: has the request finished?"""
+        d = C.c_int()
+        _check(lib().tos_server_poll(self.server._h, self.id, C.byref(d)))
+        return bool(d.value)
 
     def wait(self):
         bins = np.zeros(self.nbins, dtype=XIBIN_DTYPE)
