@@ -50,15 +50,41 @@ __device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, 
   for (int f = 0; f < 8; ++f) acc.s0[f] = acc.s1[f] = 0.0;
   unsigned rech = 0;
   unsigned long long n_eval = 0;
+  // Rows where some task of the group has a non-empty run.  Table entries are
+  // non-decreasing along the rows, so the run of (side, k) is non-empty on
+  // one row interval: side 0 [Q_k, Q_k+1) needs Q_k+1 > fj and Q_k < fj + nj,
+  // side 1 [Q_k+1, Q_k) needs Q_k > fj and Q_k+1 < fj + nj.
+  int g_lo = r_hi, g_hi = r_lo;
+  if (act) {
+    const int lo_col = side ? 0 : 1, hi_col = side ? 1 : 0;
+    int a = r_lo, b = r_hi;  // first row with Q[lo_col] > fj
+    while (a < b) {
+      const int mid = (a + b) >> 1;
+      if ((int)qrow[(size_t)mid * qstride + lo_col] > fj) b = mid; else a = mid + 1;
+    }
+    int c2 = a, d2 = r_hi;  // first row with Q[hi_col] >= fj + nj
+    while (c2 < d2) {
+      const int mid = (c2 + d2) >> 1;
+      if ((int)qrow[(size_t)mid * qstride + hi_col] >= fj + nj) d2 = mid; else c2 = mid + 1;
+    }
+    g_lo = a;
+    g_hi = c2;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    g_lo = min(g_lo, __shfl_xor_sync(kFull, g_lo, o));
+    g_hi = max(g_hi, __shfl_xor_sync(kFull, g_hi, o));
+  }
+  if (g_hi <= g_lo) return;  // warp-uniform: every run of the group is empty
   // boundaries loaded one row ahead
-  const int r0 = min(r_lo + phase, r_hi - 1);
+  const int r0 = min(g_lo + phase, g_hi - 1);
   ushort2 nQ = make_ushort2(qrow[(size_t)r0 * qstride], qrow[(size_t)r0 * qstride + 1]);
   RowV nR = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, r0);
 #pragma unroll 1
-  for (int r = r_lo + phase; r < r_hi; r += P) {
+  for (int r = g_lo + phase; r < g_hi; r += P) {
     const ushort2 Qv = nQ;
     const RowV R = nR;
-    const int rn = min(r + P, r_hi - 1);
+    const int rn = min(r + P, g_hi - 1);
     nQ = make_ushort2(qrow[(size_t)rn * qstride], qrow[(size_t)rn * qstride + 1]);
     nR = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, rn);
     const int qa = min(max((int)Qv.x - fj, 0), nj), qb = min(max((int)Qv.y - fj, 0), nj);
