@@ -122,18 +122,39 @@ __global__ void __launch_bounds__(kBruteWarps * 32, 1) brute_kernel(BruteArgs A)
     uint32_t cur = 0xFFFFFFFFu;
     int run_start = 0;
     double ps0 = 0, ps1 = 0;
-    auto close_run = [&](int p_end, double2 pn) {
-      const uint32_t m = (uint32_t)(p_end - run_start);
+    // Add the runs that lanes with `emit` close (bin `slot`, its words):
+    // lanes closing a run in the same bin, which on a regular grid is most
+    // of the warp (one separation vector per step), sum their words with
+    // redux.sync and one of them adds the sums to the window.
+    auto emit_runs = [&](bool emit, uint32_t slot, const uint32_t (&wv)[5]) {
+      unsigned pending = __ballot_sync(kFull, emit);
+      while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const uint32_t ls = __shfl_sync(kFull, slot, leader);
+        const unsigned peers = __ballot_sync(kFull, ((pending >> lane) & 1u) && slot == ls);
+        if ((peers >> lane) & 1u) {
+          uint32_t sw[5];
+#pragma unroll
+          for (int w = 0; w < 5; ++w) sw[w] = __reduce_add_sync(peers, wv[w]);
+          if (lane == leader) {
+#pragma unroll
+            for (int w = 0; w < 5; ++w) atomicAdd(&win[w * S + ls], sw[w]);
+            const uint32_t n = (uint32_t)__popc(peers);
+            const uint32_t old = atomicAdd(&win[5 * S + ls], n);
+            if (old + n > kSlotLimit) full = true;
+          }
+        }
+        pending &= ~peers;
+      }
+    };
+    auto run_words = [&](int p_end, double2 pn, uint32_t (&wv)[5]) {
       const double c0 = wdi * (pn.x - ps0), c1 = wi * (pn.y - ps1);
       const long long q0 = to_fixed(c0, A.scale[0]), q1 = to_fixed(c1, A.scale[1]);
-      const int s = (int)cur;
-      atomicAdd(&win[0 * S + s], (uint32_t)q0 & ((1u << kBSplit) - 1u));
-      atomicAdd(&win[1 * S + s], (uint32_t)(int)(q0 >> kBSplit));
-      atomicAdd(&win[2 * S + s], (uint32_t)q1 & ((1u << kBSplit) - 1u));
-      atomicAdd(&win[3 * S + s], (uint32_t)(int)(q1 >> kBSplit));
-      atomicAdd(&win[4 * S + s], m);
-      const uint32_t old = atomicAdd(&win[5 * S + s], 1u);
-      if (old >= kSlotLimit) full = true;
+      wv[0] = (uint32_t)q0 & ((1u << kBSplit) - 1u);
+      wv[1] = (uint32_t)(int)(q0 >> kBSplit);
+      wv[2] = (uint32_t)q1 & ((1u << kBSplit) - 1u);
+      wv[3] = (uint32_t)(int)(q1 >> kBSplit);
+      wv[4] = (uint32_t)(p_end - run_start);
     };
     for (int t = i0 + 1; t < A.n; ++t) {
       const int j = t + lane;
@@ -160,26 +181,32 @@ __global__ void __launch_bounds__(kBruteWarps * 32, 1) brute_kernel(BruteArgs A)
       }
       const bool change = (key != cur) || (cur != 0xFFFFFFFFu && j - run_start >= kRunCap);
       if (__any_sync(kFull, change)) {
+        uint32_t wv[5] = {0u, 0u, 0u, 0u, 0u};
+        const bool emit = change && cur != 0xFFFFFFFFu;
+        const uint32_t slot = cur;
         if (change) {
           const int pc = min(j, A.n);
           const double2 pn = A.prefix[pc];
-          if (cur != 0xFFFFFFFFu) close_run(j, pn);
+          if (emit) run_words(j, pn, wv);
           cur = key;
           run_start = j;
           ps0 = pn.x;
           ps1 = pn.y;
         }
+        emit_runs(emit, slot, wv);
         if (__any_sync(kFull, full)) {
           flush(A, win, lane);
           full = false;
         }
       }
     }
-    if (cur != 0xFFFFFFFFu) {
-      const int p_end = min(A.n - 1 + lane + 1, A.n);  // last j visited was n-1 (or earlier)
+    {
       // the sweep ended at t = n-1, so lane's last j = n-1+lane; runs only
-      // cover real points, hence end = min(n, n-1+lane+1) = n for every lane
-      close_run(p_end, A.prefix[p_end]);
+      // cover real points, hence every open run ends at n
+      uint32_t wv[5] = {0u, 0u, 0u, 0u, 0u};
+      const bool emit = cur != 0xFFFFFFFFu;
+      if (emit) run_words(A.n, A.prefix[A.n], wv);
+      emit_runs(emit, cur, wv);
     }
     if (__any_sync(kFull, full)) {
       flush(A, win, lane);
