@@ -537,7 +537,8 @@ def jackknife_measure(eng, cat, W, plain_step_s, plain_bins):
                    "on the catalogue without that region's sightlines"}
 
 
-def serving_measure(W, n_requests, serve_max, slots_list=(4, 1)):
+def serving_measure(W, n_requests, serve_max,
+                    runs=(("fifo", 4), ("shortest", 4), ("shortest", 1), ("fifo", 1))):
     """The serving pattern on a resident pool: 6 catalogues whose sightline
     counts are drawn log-uniform in [1k, 160k] and capped at serve_max (the
     first N sightlines of the full-survey catalogue, a uniform subsample of
@@ -545,8 +546,8 @@ def serving_measure(W, n_requests, serve_max, slots_list=(4, 1)):
     time), requests arriving as a
     Poisson stream at 20/s, each for a pool catalogue at random with
     (r_par,r_perp) 50x50 or (r,mu) 50x20 binning at random, admitted under a
-    150 GB budget.  Run once with several slots (continuous admission) and
-    once with one slot (one request at a time)."""
+    150 GB budget.  Run with several slots (continuous admission) in arrival
+    order and least-work-first, and with one slot (one request at a time)."""
     import threading
 
     import tos_b200 as T
@@ -562,8 +563,9 @@ def serving_measure(W, n_requests, serve_max, slots_list=(4, 1)):
                        f"[1k,160k] capped at {serve_max}), Poisson arrivals at 20/s, binning (r_par,r_perp) "
                        "50x50 or (r,mu) 50x20 at random, 150 GB budget, FIFO admission",
            "pool_sightlines": [int(c) for c in counts], "requests": int(n_requests)}
-    for slots in slots_list:
+    for policy, slots in runs:
         srv = T.Server(0, slots=slots, memory_budget_bytes=150 * 10**9)
+        srv.set_policy(policy, max_wait_s=5.0)
         eng = T.Engine(0)
         pool = []
         for n in counts:
@@ -600,7 +602,7 @@ def serving_measure(W, n_requests, serve_max, slots_list=(4, 1)):
             c.close()
         eng.close()
         span = last - first
-        out[f"slots_{slots}"] = {"value": pairs / span, "unit": UNIT, "makespan_s": span,
+        out[f"{policy}_slots_{slots}"] = {"value": pairs / span, "unit": UNIT, "makespan_s": span,
                                  "p50_latency_s": float(np.percentile(lat, 50)),
                                  "p99_latency_s": float(np.percentile(lat, 99)),
                                  "pixel_pairs": pairs, "peak_device_bytes": int(status["peak_bytes"])}

@@ -294,6 +294,13 @@ tos_status tos_server_submit(tos_server* server, tos_catalog* catalog, const tos
  * its flags ask for (NULL to drop them), stats and info optional. */
 tos_status tos_server_wait(tos_server* server, uint64_t request_id, tos_xibin* out_bins,
                            tos_xibin* out_rows, tos_xi_stats* stats, tos_request_info* info);
+/* Admission order of queued requests: TOS_SERVER_FIFO (arrival order, the
+ * default) or TOS_SERVER_SHORTEST (least estimated pixel pairs first; a
+ * request that has waited more than max_wait_s seconds goes first and is not
+ * overtaken, so none waits forever behind smaller ones). */
+#define TOS_SERVER_FIFO 0
+#define TOS_SERVER_SHORTEST 1
+tos_status tos_server_set_policy(tos_server* server, int policy, double max_wait_s);
 /* Non-blocking: *done = 1 when the request has finished (tos_server_wait then
  * returns at once), 0 while it is queued or running. */
 tos_status tos_server_poll(tos_server* server, uint64_t request_id, int* done);

@@ -2,6 +2,7 @@
 // host logic only, built and run by tests/test_admission.py.
 #include <cstdio>
 #include <cstdlib>
+#include <vector>
 
 #include "admission.h"
 
@@ -78,6 +79,20 @@ int main() {
     CHECK(!a.can_ever_fit(91));
     CHECK(a.pick(91) < 0);
     CHECK(a.trim_victim(91) < 0);
+  }
+  {  // admission order
+    using tos::order_queue;
+    std::vector<bool> strict;
+    const std::vector<tos::QueuedView> q = {{9e12, 0.5}, {1e10, 0.2}, {4e11, 0.1}, {2e12, 7.0}};
+    std::vector<size_t> o = order_queue(q, tos::kFifo, 5.0, &strict);
+    CHECK(o.size() == 1 && o[0] == 0 && strict[0]);  // FIFO: the head only
+    o = order_queue(q, tos::kShortest, 5.0, &strict);
+    CHECK(o.size() == 4);
+    CHECK(o[0] == 3 && strict[0]);                    // waited 7 s > 5 s: first, not overtaken
+    CHECK(o[1] == 1 && o[2] == 2 && o[3] == 0);       // then least work first
+    CHECK(!strict[1] && !strict[2] && !strict[3]);
+    o = order_queue({}, tos::kShortest, 5.0, &strict);
+    CHECK(o.empty());
   }
   std::puts("admission: ok");
   return 0;

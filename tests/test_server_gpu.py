@@ -5,7 +5,9 @@ Pass criteria: every request's result is bit-identical to tos_xi_run on the
 same catalogue alone (bins, per-group rows, pair counts), whatever else runs
 beside it; requests on different slots overlap in time; under a budget that
 holds one workspace at a time they run one after another and still give the
-same results; requests and catalogues that cannot fit are refused."""
+same results; FIFO starts requests in arrival order, shortest-first may
+reorder them but gives the same results; requests and catalogues that
+cannot fit are refused."""
 import numpy as np
 import pytest
 
@@ -57,11 +59,13 @@ def assert_identical(x, y, what):
         assert np.array_equal(x[f], y[f]), f"{what}: field {f} differs"
 
 
-def test_results_same_alone_and_in_mix(engine, catalogs):
+@pytest.mark.parametrize("policy", ["fifo", "shortest"])
+def test_results_same_alone_and_in_mix(engine, catalogs, policy):
     ref = {}
     for key, gname, pg in mix():
         ref[(key, gname, pg)] = alone(engine, catalogs, key, gname, pg)
     with T.Server(0, slots=3, memory_budget_bytes=40 * 10**9) as srv:
+        srv.set_policy(policy, max_wait_s=5.0)
         for cat, _ in catalogs.values():
             srv.attach(cat)
         reqs = []
@@ -91,6 +95,9 @@ def test_results_same_alone_and_in_mix(engine, catalogs):
     assert most >= 2
     for i in infos:
         assert i["submit_s"] <= i["start_s"] <= i["end_s"]
+    if policy == "fifo":  # requests start in arrival order
+        starts = [i["start_s"] for i in infos]
+        assert starts == sorted(starts)
 
 
 def test_budget_for_one_workspace_serialises(engine, catalogs):

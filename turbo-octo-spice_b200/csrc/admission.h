@@ -6,18 +6,53 @@
 // steady stream of requests allocates nothing); a request that needs more
 // grows it.  A request may start on a free slot k when
 //     resident + sum_{s != k} held[s] + max(held[k], need) <= budget.
-// Requests start in arrival order (FIFO).  When the head of the queue fits
-// on no free slot, idle slots give their workspaces back (largest first)
-// until it fits; if it still does not fit it waits for running requests to
-// finish.  A request that cannot fit even with every slot empty is refused
+// Requests start in arrival order (FIFO), or least estimated work first with
+// aging (order_queue).  When the first candidate fits on no free slot, idle
+// slots give their workspaces back (largest first) until it fits; if it
+// still does not fit it waits for running requests to finish.  A request that cannot fit even with every slot empty is refused
 // at submission.
 #pragma once
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <vector>
 
 namespace tos {
+
+// Order in which queued requests are offered to the slots.
+enum QueuePolicy {
+  kFifo = 0,      // arrival order; the head waits until it fits (no overtaking)
+  kShortest = 1,  // smallest estimated work first; a request waiting longer than
+                  // max_wait_s goes first (oldest first) and is not overtaken
+};
+
+struct QueuedView {
+  double work;      // estimated pixel pairs
+  double waited_s;  // time in the queue
+};
+
+// Candidates to start, in preference order, as positions in the queue
+// (arrival order).  The first candidate that fits starts; a candidate marked
+// strict in `strict` stops the search when it does not fit.
+inline std::vector<size_t> order_queue(const std::vector<QueuedView>& q, int policy,
+                                       double max_wait_s, std::vector<bool>* strict) {
+  std::vector<size_t> idx(q.size());
+  for (size_t k = 0; k < q.size(); ++k) idx[k] = k;
+  strict->assign(q.size(), true);
+  if (policy == kFifo || q.empty()) {
+    idx.resize(q.empty() ? 0 : 1);
+    return idx;
+  }
+  std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+    const bool oa = q[a].waited_s > max_wait_s, ob = q[b].waited_s > max_wait_s;
+    if (oa != ob) return oa;                       // waited too long: first
+    if (oa) return q[a].waited_s > q[b].waited_s;  // ... oldest first
+    return q[a].work < q[b].work;                  // then the least work
+  });
+  for (size_t k = 0; k < idx.size(); ++k) (*strict)[k] = q[idx[k]].waited_s > max_wait_s;
+  return idx;
+}
 
 class Admission {
  public:

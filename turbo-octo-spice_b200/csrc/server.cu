@@ -38,6 +38,8 @@ struct Request {
   double scale = 0;
   uint32_t flags = 0;
   uint64_t need = 0;   // workspace estimate (bytes)
+  double work = 0;     // estimated pixel pairs (admission order)
+  double t_submit = 0; // server clock at submission
   size_t n_rows = 0;   // per-cell or per-group rows returned
   std::vector<tos_xibin> bins, rows;
   tos_xi_stats stats{};
@@ -49,9 +51,19 @@ struct Request {
 
 constexpr double kPi = 3.14159265358979323846;
 
-// Device bytes a run of `cat` on grid g needs in a workspace.  The sightline
-// pairs are estimated for a uniform sky density over the occupied cells
-// (pairs ~ N^2 / 2 * disc / area, with a 1.5 margin); the rest is exact.
+// Device bytes a run of `cat` on grid g needs in a workspace: the sightline
+// pairs are pairs_estimate's, the rest is exact.
+// Estimated sightline pairs of a run (uniform sky density over the occupied
+// cells, with a 1.5 margin).
+double pairs_estimate(const tos_catalog* cat, const tos_grid& g, double scale) {
+  const double nc = (double)cat->cells.size(), n = (double)cat->n_los;
+  const double cell_sr = 4.0 * kPi / (12.0 * (double)cat->nside * (double)cat->nside);
+  const double area = std::max(nc * cell_sr, cell_sr);
+  const double ang = std::min(max_angular_scale(g, scale), kPi);
+  const double disc = 2.0 * kPi * (1.0 - std::cos(ang));
+  return 1.5 * 0.5 * n * std::min(n, n * disc / area) + n;
+}
+
 uint64_t workspace_estimate(const tos_catalog* cat, const tos_grid& g, double scale, size_t n_rows) {
   const double nb = (double)g.axis[0].nbins * g.axis[1].nbins * g.axis[2].nbins;
   const double nc = (double)cat->cells.size(), n = (double)cat->n_los;
@@ -59,8 +71,7 @@ uint64_t workspace_estimate(const tos_catalog* cat, const tos_grid& g, double sc
   const double area = std::max(nc * cell_sr, cell_sr);
   const double ang = std::min(max_angular_scale(g, scale), kPi);
   const double disc = 2.0 * kPi * (1.0 - std::cos(ang));
-  const double partners = std::min(n, n * disc / area);
-  const double pairs = 1.5 * 0.5 * n * partners + n;
+  const double pairs = pairs_estimate(cat, g, scale);
   const double near_cells = std::min(nc, nc * disc / area + 9.0);
   double bytes = 0;
   bytes += nc * nb * 128.0;                                   // per-cell sums
@@ -91,6 +102,8 @@ struct tos_server {
   std::unordered_map<uint64_t, std::unique_ptr<tos::Request>> reqs;
   std::unordered_map<const tos_catalog*, uint64_t> attached;  // catalogue -> resident bytes
   std::unordered_map<const tos_catalog*, uint64_t> pending;   // unfinished requests per catalogue
+  int policy = tos::kFifo;
+  double max_wait_s = 5.0;
   uint64_t next_id = 1, completed = 0, peak = 0;
   bool stop = false;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -99,13 +112,26 @@ struct tos_server {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
 
-  // Start queued requests while the head fits (mu held).
+  // Start queued requests while a candidate fits (mu held).
   void dispatch() {
     while (!queue.empty()) {
-      tos::Request* r = queue.front();
-      const int k = adm.pick(r->need);
+      const double t = now();
+      std::vector<tos::QueuedView> view(queue.size());
+      for (size_t q = 0; q < queue.size(); ++q) view[q] = {queue[q]->work, t - queue[q]->t_submit};
+      std::vector<bool> strict;
+      const std::vector<size_t> order = tos::order_queue(view, policy, max_wait_s, &strict);
+      size_t pos = queue.size();
+      int k = -1;
+      for (size_t c = 0; c < order.size(); ++c) {
+        k = adm.pick(queue[order[c]]->need);
+        if (k >= 0) {
+          pos = order[c];
+          break;
+        }
+        if (strict[c]) break;  // not overtaken
+      }
       if (k < 0) {
-        const int v = adm.trim_victim(r->need);
+        const int v = adm.trim_victim(queue[order[0]]->need);
         if (v < 0) break;  // wait for a running request to finish
         // an idle slot gives its workspace back (its stream has no work)
         int prev = -1;
@@ -116,7 +142,8 @@ struct tos_server {
         adm.release(v);
         continue;
       }
-      queue.pop_front();
+      tos::Request* r = queue[pos];
+      queue.erase(queue.begin() + (long)pos);
       adm.start(k, r->need);
       peak = std::max(peak, adm.in_use());
       r->info.start_s = now();
@@ -272,6 +299,10 @@ tos_status tos_server_submit(tos_server* s, tos_catalog* cat, const tos_grid* gr
               : (flags & TOS_XI_PER_GROUP) ? cat->groups.size()
                                            : 0;
   r->need = workspace_estimate(cat, *grid, scale, r->n_rows);
+  {
+    const double px = (double)cat->n_pix / std::max<double>(1.0, (double)cat->n_los);
+    r->work = pairs_estimate(cat, *grid, scale) * px * px;
+  }
   r->info.workspace_bytes = r->need;
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return fail(TOS_ERR_INVALID_ARG, "server is shutting down");
@@ -282,6 +313,7 @@ tos_status tos_server_submit(tos_server* s, tos_catalog* cat, const tos_grid* gr
                                  "resident catalogues");
   r->id = s->next_id++;
   r->info.submit_s = s->now();
+  r->t_submit = r->info.submit_s;
   r->info.slot = -1;
   *request_id = r->id;
   s->pending[cat]++;
@@ -309,6 +341,17 @@ tos_status tos_server_wait(tos_server* s, uint64_t id, tos_xibin* out_bins, tos_
   if (out_bins) std::copy(r->bins.begin(), r->bins.end(), out_bins);
   if (out_rows && r->n_rows) std::copy(r->rows.begin(), r->rows.end(), out_rows);
   if (stats) *stats = r->stats;
+  return TOS_OK;
+}
+
+tos_status tos_server_set_policy(tos_server* s, int policy, double max_wait_s) {
+  if (!s) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (policy != kFifo && policy != kShortest) return fail(TOS_ERR_INVALID_ARG, "unknown policy");
+  if (!(max_wait_s >= 0)) return fail(TOS_ERR_INVALID_ARG, "max_wait_s must be >= 0");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->policy = policy;
+  s->max_wait_s = max_wait_s;
+  s->dispatch();
   return TOS_OK;
 }
 

@@ -122,6 +122,7 @@ def lib() -> C.CDLL:
         L.tos_server_wait.argtypes = [vp, u64, vp, vp, C.POINTER(XiStats), C.POINTER(RequestInfo)]
         L.tos_server_status_get.argtypes = [vp, C.POINTER(ServerStatus)]
         L.tos_server_poll.argtypes = [vp, u64, C.POINTER(C.c_int)]
+        L.tos_server_set_policy.argtypes = [vp, i32, dbl]
         L.tos_catalog_device_bytes.argtypes = [vp, C.POINTER(u64)]
         L.tos_comoving_distance.argtypes = [dbl, vp, sz, vp]
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
@@ -348,6 +349,11 @@ class Server:
 
     def attach(self, catalog: Catalog):
         _check(lib().tos_server_attach(self._h, catalog.handle))
+
+    def set_policy(self, policy: str = "fifo", max_wait_s: float = 5.0):
+        """Admission order: "fifo" (arrival order) or "shortest" (least
+        estimated work first, with requests older than max_wait_s first)."""
+        _check(lib().tos_server_set_policy(self._h, {"fifo": 0, "shortest": 1}[policy], max_wait_s))
 
     def detach(self, catalog: Catalog):
         _check(lib().tos_server_detach(self._h, catalog.handle))
