@@ -245,6 +245,16 @@ tos_status tos_xi_run_jackknife(tos_engine* engine, tos_catalog* catalog, const 
                                 size_t* n_regions, int64_t* region_ids, tos_xibin* out_bins,
                                 tos_xibin* out_groups, tos_xibin* out_drop, tos_xi_stats* stats);
 
+/* Jackknife covariance of n_rows delete-one subsamples, such as the out_drop
+ * rows of one group from tos_xi_run_jackknife: xi_k[b] = didj/wgt (0 where
+ * wgt <= 0), mean = sum_k xi_k / N and cov = (N - 1)/N sum_k (xi_k - mean)
+ * (xi_k - mean)^T (n_bins x n_bins, row-major; N = n_rows >= 2), the
+ * estimator tos_xi_jackknife applies to its region estimates.  xi (n_rows x
+ * n_bins) and mean may be NULL.  No counterpart in the reference, which
+ * leaves subsample covariances to likely (XiEstimator.cc:60-97). */
+tos_status tos_xi_subsample_covariance(tos_engine* engine, const tos_xibin* rows, size_t n_rows,
+                                       size_t n_bins, double* xi, double* mean, double* cov);
+
 /* XiBin::finalize (types.h:96-101) applied to n bins in place. */
 void tos_xibin_finalize(tos_xibin* bins, size_t n);
 

@@ -114,3 +114,24 @@ def test_jackknife_run_arguments(engine):
     with pytest.raises(T.TosError):
         T.cell_covariance(engine, cat, g.nbins)
     cat.close()
+
+
+def test_subsample_covariance(engine):
+    """The jackknife covariance of the one-pass subsamples against numpy:
+    xi_k = didj/wgt (0 where wgt <= 0), cov = (N-1)/N sum (xi_k - mean)^T (xi_k - mean),
+    to 1e-10 of the largest |cov| entry (FP64, different summation order)."""
+    g = GRIDS["cartesian"]
+    los, px, meta = small_catalog(n=200, seed=6, size_deg=8.0, max_pixels=120)
+    cat = T.Catalog(engine, los, px, ORDER)
+    ids, bins, groups, drop, st = T.xi_run_jackknife(engine, cat, g, meta["scale"], REGION_ORDER)
+    cat.close()
+    xi, mean, cov = T.subsample_covariance(engine, drop)
+    wgt = drop["wgt"].astype(np.float64)
+    X = np.where(wgt > 0, drop["didj"] / np.where(wgt > 0, wgt, 1.0), 0.0)
+    assert np.array_equal(xi, X)
+    n = len(ids)
+    m = X.mean(axis=0)
+    C = (n - 1) / n * (X - m).T @ (X - m)
+    assert np.allclose(mean, m, rtol=0, atol=1e-12 * np.abs(m).max())
+    assert np.abs(cov - C).max() <= 1e-10 * np.abs(C).max()
+    assert np.allclose(cov, cov.T, rtol=0, atol=1e-12 * np.abs(C).max())

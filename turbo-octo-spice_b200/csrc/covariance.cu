@@ -289,3 +289,26 @@ extern "C" tos_status tos_xi_jackknife(tos_engine* e, tos_catalog* cat, int regi
   return sample_covariance(e, dX.p, nullptr, (uint32_t)nr, nb, (double)nr, (double)(nr - 1) / (double)nr,
                            nullptr, cov);
 }
+
+extern "C" tos_status tos_xi_subsample_covariance(tos_engine* e, const tos_xibin* rows,
+                                                  size_t n_rows, size_t n_bins, double* xi,
+                                                  double* mean, double* cov) {
+  if (!e || !rows || !cov) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (n_rows < 2) return fail(TOS_ERR_INVALID_ARG, "need at least two subsamples");
+  if (n_bins < 1 || n_bins > 65536 || n_rows > 0xFFFFFFFFull)
+    return fail(TOS_ERR_INVALID_ARG, "n_bins must be in [1, 65536]");
+  // xi_k[b] = didj / wgt, 0 where wgt <= 0 (as the per-cell samples)
+  std::vector<double> X(n_rows * n_bins);
+  for (size_t k = 0; k < n_rows * n_bins; ++k)
+    X[k] = rows[k].wgt > 0 ? rows[k].didj / rows[k].wgt : 0.0;
+  if (xi) std::copy(X.begin(), X.end(), xi);
+  std::lock_guard<std::mutex> lock(e->mu);
+  DevGuard g(e->device);
+  DevBuf<double> dX;
+  TOS_TRY(dX.alloc(X.size()));
+  TOS_CUDA_TRY(cudaMemcpyAsync(dX.p, X.data(), X.size() * 8, cudaMemcpyHostToDevice, e->stream));
+  const double n = (double)n_rows;
+  // C = (N - 1)/N sum_k (xi_k - mean)(xi_k - mean)^T
+  return sample_covariance(e, dX.p, nullptr, (uint32_t)n_rows, (uint32_t)n_bins, n, (n - 1.0) / n,
+                           mean, cov);
+}

@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         L.tos_brute_run_noalloc.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
         L.tos_xi_cell_covariance.argtypes = [vp, vp, vp, vp, vp]
         L.tos_xi_jackknife.argtypes = [vp, vp, i32, sz, C.POINTER(sz), vp, vp, vp]
+        L.tos_xi_subsample_covariance.argtypes = [vp, vp, sz, sz, vp, vp, vp]
         L.tos_xi_run_jackknife.argtypes = [vp, vp, C.POINTER(_Grid), dbl, u32, i32, sz, C.POINTER(sz),
                                            vp, vp, vp, vp, C.POINTER(XiStats)]
         L.tos_server_create.argtypes = [i32, i32, u64, C.POINTER(vp)]
@@ -410,6 +411,18 @@ class ServerRequest:
         _check(lib().tos_server_wait(self.server._h, self.id, _ptr(bins),
                                      _ptr(rows) if rows is not None else None, C.byref(st), C.byref(info)))
         return bins, rows, st.as_dict(), info.as_dict()
+
+
+def subsample_covariance(engine: Engine, rows: np.ndarray):
+    """Jackknife covariance of delete-one subsample rows (n, nbins) XiBin
+    arrays, e.g. one group's rows of xi_run_jackknife.  Returns (xi, mean, cov)."""
+    rows = np.ascontiguousarray(rows, dtype=XIBIN_DTYPE)
+    n, nb = rows.shape
+    xi = np.zeros((n, nb))
+    mean = np.zeros(nb)
+    cov = np.zeros((nb, nb))
+    _check(lib().tos_xi_subsample_covariance(engine.handle, _ptr(rows), n, nb, _ptr(xi), _ptr(mean), _ptr(cov)))
+    return xi, mean, cov
 
 
 def finalize(bins: np.ndarray) -> np.ndarray:
