@@ -150,3 +150,16 @@ def test_refusals(engine, catalogs):
         with pytest.raises(T.TosError):
             r.done()  # the id is released by wait
         srv.detach(cat)
+
+
+def test_destroy_with_requests_in_flight(engine, catalogs):
+    """Destroying a server finishes the running request and ends the queued
+    ones; nothing hangs and the ids are gone afterwards."""
+    cat, scale = catalogs["b"]
+    srv = T.Server(0, slots=1, memory_budget_bytes=40 * 10**9)
+    srv.attach(cat)
+    reqs = [srv.submit(cat, GRIDS["polar"], scale) for _ in range(4)]
+    srv.close()  # joins the running request, drops the three queued ones
+    for r in reqs:
+        with pytest.raises(T.TosError):
+            r.wait()  # the server handle is gone: a clean error, not a crash
