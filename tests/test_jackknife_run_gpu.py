@@ -12,7 +12,7 @@ import pytest
 
 import tos_b200 as T
 from tos_b200 import synth  # noqa: F401  (T.synth)
-from helpers import FIELDS, GRIDS, assert_same_count, small_catalog
+from helpers import FIELDS, GRIDS, assert_counts_equal, assert_same_count, assert_sums_close, small_catalog
 from oracle import oracle
 
 pytestmark = pytest.mark.gpu
@@ -135,3 +135,24 @@ def test_subsample_covariance(engine):
     assert np.allclose(mean, m, rtol=0, atol=1e-12 * np.abs(m).max())
     assert np.abs(cov - C).max() <= 1e-10 * np.abs(C).max()
     assert np.allclose(cov, cov.T, rtol=0, atol=1e-12 * np.abs(C).max())
+
+
+def test_jackknife_run_exact_path(engine):
+    """TOS_XI_EXACT (every pixel pair in FP64, the pixel-pair kernel's direct
+    adds on the 42-bit scale of positive fields) routes pairs to the same
+    region slots: identical pair counts per subsample, and sums within
+    REL_TOL of the FP64 oracle."""
+    g = GRIDS["cartesian"]
+    los, px, meta = small_catalog(n=120, seed=12, size_deg=6.0, max_pixels=80)
+    cat = T.Catalog(engine, los, px, ORDER)
+    ids, bins, _, drop, _ = T.xi_run_jackknife(engine, cat, g, meta["scale"], REGION_ORDER)
+    ids2, bins2, _, drop2, st2 = T.xi_run_jackknife(engine, cat, g, meta["scale"], REGION_ORDER, exact=True)
+    cat.close()
+    assert st2["num_run_items"] == 0
+    assert np.array_equal(ids, ids2)
+    assert_counts_equal(bins2, bins)
+    ob = oracle.xi(los, px, ORDER, g.type, g.axes_array(), meta["scale"], mode=1)[0]
+    assert_counts_equal(bins2, ob)
+    assert_sums_close(bins2, ob, abs_sums(los, px, g, meta["scale"]))
+    for k in range(len(ids)):
+        assert np.array_equal(drop2[k]["num_pairs"], drop[k]["num_pairs"])

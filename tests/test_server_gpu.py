@@ -163,3 +163,17 @@ def test_destroy_with_requests_in_flight(engine, catalogs):
     for r in reqs:
         with pytest.raises(T.TosError):
             r.wait()  # the server handle is gone: a clean error, not a crash
+
+
+def test_subsample_rows_through_the_server(engine, catalogs):
+    """A request for per-cell rows returns tos_xi_run's per-cell sums."""
+    cat, scale = catalogs["a"]
+    g = GRIDS["cartesian"]
+    rb, rc, _ = T.xi_run(engine, cat, g, scale, subsamples=True)
+    with T.Server(0, slots=2, memory_budget_bytes=10**10) as srv:
+        srv.attach(cat)
+        bins, rows, _, _ = srv.submit(cat, g, scale, subsamples=True).wait()
+    assert rows.shape == rc.shape
+    assert_identical(bins, rb, "bins")
+    for c in range(rows.shape[0]):
+        assert_identical(rows[c], rc[c], f"cell {c}")
