@@ -34,7 +34,7 @@ namespace tos {
 
 constexpr uint32_t kInvalidKey = 0xFFFFFFFFu;
 constexpr uint32_t kNoGrid = 0xFFFFFFFFu;  // sightline not contiguous on the common grid
-constexpr int kPairWarps = 12;  // warps per CTA of the pair kernel
+constexpr int kPairWarps = 16;  // warps per CTA of the pair kernel
 // u32 words per window slot: the three signed sums (didj, di, dj) as 22+22+rest
 // bit words of a 62-bit fixed-point value, the four positive sums (wgt, wi,
 // wj, z) as 22+rest bit words of a 42-bit value, the pair count and the
