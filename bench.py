@@ -63,8 +63,11 @@ def parse():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--workload", choices=["full", "small", "brute"], default="full")
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--cpu-seconds", type=float, default=18.0, help="target CPU-baseline sample time")
+    ap.add_argument("--cpu-cells", type=int, default=40,
+                    help="CPU legs: primary cells of the seeded sample the reference path is timed on")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the check of 24 primary cells against the reference and the FP64 oracle")
     ap.add_argument("--sightlines", type=int, default=160000,
                     help="full workload: sightlines over the same ~10000 deg^2 (profiling uses fewer)")
     ap.add_argument("--grid", choices=["cartesian", "polar"], default="cartesian",
@@ -207,69 +210,157 @@ def make_workload(kind, n_full=160000, binning="cartesian"):
 
 
 # ---------------------------------------------------------------- CPU baseline
-def cpu_sample(W, seconds, nthreads):
-    """Time the reference algorithm (oracle, reference build flags) on a
-    bounded sample of primary cells; returns (pixel_pairs/s, sample description)."""
+def sample_cells(W, n_cells, seed=0):
+    """A seeded sample of n_cells occupied HEALPix cells (ids ascending) and
+    their positions among the occupied cells: the primary cells both CPU legs
+    time, chosen from the sightline positions alone."""
+    from oracle import oracle
+    order = W["order"]
+    cells = np.array([oracle.radec2pix(order, float(r), float(d)) for r, d in zip(W["los"]["ra"], W["los"]["dec"])])
+    occupied = np.unique(cells)
+    rng = np.random.default_rng(seed)
+    pos = np.sort(rng.choice(len(occupied), size=min(n_cells, len(occupied)), replace=False))
+    return occupied[pos], pos
+
+
+def cpu_sample(W, nthreads, n_cells=40):
+    """Time the reference's CPU path on a bounded sample of the workload;
+    returns (pixel pairs/s, kind, sample description).  XiEstimator workloads:
+    the reference's own XiEstimator::run (oracle/_ref/libtosref_fast.so,
+    built from its sources with its -O3 -ffast-math) over a seeded sample of
+    primary cells, timed around run() alone; where that build is absent, the
+    oracle port with the same flags on the same cells.  Brute workload: the
+    oracle port of the FP64 all-pairs loop (the reference's CPU estimator,
+    bucketxi, bins in two dimensions) on the first rows of the grid."""
     from oracle import oracle
     if "pts" in W:
         pts = W["pts"]
-        # rows [0, m) against all later rows: the first m*(n - (m+1)/2) pairs
         n = len(pts)
-        m = 256
-        t = time.perf_counter()
-        oracle.brute(pts[: min(n, 4096)], 0.0, 200.0, 100, nthreads=nthreads, kind="fast")
-        dt = time.perf_counter() - t
-        npairs = min(n, 4096) * (min(n, 4096) - 1) // 2
-        rate = npairs / dt
-        sub = int(min(n, max(4096, math.sqrt(2 * rate * seconds))))
+        sub = min(n, 24576)
         t = time.perf_counter()
         oracle.brute(pts[:sub], 0.0, 200.0, 100, nthreads=nthreads, kind="fast")
         dt = time.perf_counter() - t
         npairs = sub * (sub - 1) // 2
-        return npairs / dt, f"all pairs of the first {sub} grid points ({npairs} pairs), {dt:.1f} s"
+        return npairs / dt, "port", (f"all pairs of the first {sub} grid points ({npairs} pairs), {dt:.1f} s; "
+                                     "oracle/xi_oracle.c built with -O3 -ffast-math")
     g = W["grid"]
-    costs = oracle.cell_costs(W["los"], W["order"], g.type, g.axes_array(), W["scale"], kind="fast")
-    rng = np.random.default_rng(0)
-    order = np.argsort(np.abs(costs.astype(np.float64) - np.median(costs)) + rng.uniform(0, 1e-3, len(costs)))
-    # calibrate on one median cell
-    t = time.perf_counter()
-    _, _, _, st = oracle.xi(W["los"], W["px"], W["order"], g.type, g.axes_array(), W["scale"], mode=0,
-                            nthreads=nthreads, cell_subset=np.array([order[0]]), kind="fast")
-    rate1 = st["num_pixel_pairs"] / max(time.perf_counter() - t, 1e-6)  # one thread busy
-    per_cell = float(np.median(costs))
-    ncell = int(max(2 * nthreads, min(len(costs), seconds * rate1 * nthreads / max(per_cell, 1.0))))
-    subset = np.sort(order[:ncell])
-    t = time.perf_counter()
-    _, _, _, st = oracle.xi(W["los"], W["px"], W["order"], g.type, g.axes_array(), W["scale"], mode=0,
-                            nthreads=nthreads, cell_subset=subset, kind="fast")
-    dt = time.perf_counter() - t
-    desc = (f"{ncell} of {len(costs)} occupied cells (those nearest the median cost), "
-            f"{st['num_pixel_pairs']} pixel pairs, {dt:.1f} s")
-    return st["num_pixel_pairs"] / dt, desc
+    ids, pos = sample_cells(W, n_cells)
+    if oracle.ref_available("fast"):
+        _, _, _, _, st = oracle.ref_xi(W["los"], W["px"], W["order"], g.type, g.axes_array(), W["scale"],
+                                       nthreads=nthreads, cell_subset=ids, kind="fast")
+        dt = st["run_seconds"]
+        kind, what = "reference", ("the reference's XiEstimator::run (turbooctospice/XiEstimator.cc, ThreadPool.cc) "
+                                   "built unchanged with -O3 -ffast-math, timed around run()")
+    else:
+        t = time.perf_counter()
+        _, _, _, st = oracle.xi(W["los"], W["px"], W["order"], g.type, g.axes_array(), W["scale"], mode=0,
+                                nthreads=nthreads, cell_subset=pos.astype(np.uint32), kind="fast")
+        dt = time.perf_counter() - t
+        kind, what = "port", "oracle/xi_oracle.c built with -O3 -ffast-math"
+    desc = (f"{len(ids)} seeded random primary cells of {W['config']['workload'].split(':')[0]}, "
+            f"{st['num_pixel_pairs']} pixel pairs, {dt:.1f} s; {what}; {nthreads} threads")
+    return st["num_pixel_pairs"] / dt, kind, desc
+
+
+def reference_brute(args, W):
+    """Reference arm of the brute workload: the reference's own bruteGPU
+    (gpu/brute.cu, built for sm_100a into oracle/_ref/libtosref_brute.so)
+    over the whole 64^3 grid, wall time per call (its chunk loop copies from
+    the host, launches and reads back synchronously)."""
+    from oracle import oracle
+    pts = W["pts"]
+    n = len(pts)
+    pairs = n * (n - 1) // 2
+    for _ in range(args.warmup):
+        oracle.ref_brute_gpu(pts, 0.0, 200.0, 100)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        oracle.ref_brute_gpu(pts, 0.0, 200.0, 100)
+        times.append(time.perf_counter() - t)
+    value = pairs * args.steps / sum(times)
+    return value, {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"the whole grid ({pairs} pairs) per step through bruteGPU(columns, 0, 200, 100, xi, "
+                             "4096) of gpu/brute.cu built for sm_100a; wall time per call"}
 
 
 def reference_arm(args, D):
     if D.rank != 0:
         return
+    from oracle import oracle
     W = make_workload(args.workload, args.sightlines, args.grid)
     nthreads = os.cpu_count() or 1
-    per_step = max(5.0, min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup)))
-    for _ in range(args.warmup):
-        cpu_sample(W, per_step / 2, nthreads)
-    vals, descs = [], []
-    for _ in range(args.steps):
-        v, d = cpu_sample(W, per_step, nthreads)
-        vals.append(v)
-        descs.append(d)
-    value = float(np.mean(vals))
+    if "pts" in W and oracle.ref_available("brute"):
+        value, cpu = reference_brute(args, W)
+        dtype = "f32"
+    else:
+        for _ in range(args.warmup):
+            cpu_sample(W, nthreads, max(4, args.cpu_cells // 4))
+        vals = []
+        for _ in range(args.steps):
+            v, kind, desc = cpu_sample(W, nthreads, args.cpu_cells)
+            vals.append(v)
+        value = float(np.mean(vals))
+        cpu = {"value": value, "unit": UNIT, "cores": nthreads, "kind": kind, "sample": desc}
+        dtype = "f64"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": W["config"],
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": descs[-1] + "; oracle/xi_oracle.c built with -O3 -ffast-math"},
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+            "config": W["config"], "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def parity_measure(eng, cat, W, plain_bins):
+    """The checker leg, after the timed steps: one pair count with per-cell
+    results, and its rows for 24 primary cells (4 costliest, 4 at the mask
+    edge, 16 nearest the median) against the reference's own XiEstimator on
+    the same cells (pair counts bit for bit) and the FP64 oracle (sums to a
+    relative 1e-6 per bin)."""
+    import tos_b200 as T
+    from oracle import parity
+    g = W["grid"]
+    bins, rows, _ = T.xi_run(eng, cat, g, W["scale"], subsamples=True)
+    assert np.array_equal(bins["num_pairs"], plain_bins["num_pairs"])
+    ids = cat.cells()
+    pos_of = np.searchsorted(ids, cat.sightline_cells())
+    pix = np.bincount(pos_of, weights=W["los"]["num_pixels"].astype(np.float64), minlength=len(ids))
+    sel = parity.pick_cells(rows["num_pairs"].sum(axis=1), pix)
+    mine = rows[sel].copy()
+    del rows
+    t = time.perf_counter()
+    out = parity.check_cells(mine, sel, ids[sel], W["los"], W["px"], W["order"], g.type, g.axes_array(), W["scale"])
+    out["check_s"] = time.perf_counter() - t
+    out["selection"] = "4 costliest cells, 4 mask-edge cells (fewest pairs per own pixel), 16 nearest the median"
+    return out
+
+
+def brute_parity(eng, pts, m=512):
+    """The checker leg of the brute workload: the pairs (i, j) with i < m and
+    j > i, rows [0, m) of the grid against every later row.  The FP64 oracle
+    counts them directly; the engine's are the difference of its all-pairs
+    counts over the whole grid and over rows [m, n).  Counts must be equal
+    bin for bin, sums within a relative 1e-6."""
+    import tos_b200 as T
+    from oracle import oracle
+    t = time.perf_counter()
+    ref = oracle.brute_rows(pts, m, 0.0, 200.0, 100, kind="strict")
+    check_s = time.perf_counter() - t
+    e_full = T.brute_run(eng, pts, 0.0, 200.0, 100)
+    e_tail = T.brute_run(eng, pts[m:], 0.0, 200.0, 100)
+    got = [e_full[k] - e_tail[k] for k in (0, 1)] + [e_full[2].astype(np.int64) - e_tail[2].astype(np.int64)]
+    out = {"checker": "FP64 oracle (strict build), pairs of the first rows", "rows": m,
+           "pairs_compared": int(ref[2].astype(np.int64).sum()),
+           "counts_equal": bool(np.array_equal(got[2], ref[2].astype(np.int64))), "check_s": check_s}
+    errs = []
+    for k in (0, 1):
+        r, g = np.asarray(ref[k]), np.asarray(got[k])
+        nz = r != 0
+        errs.append(float(np.max(np.abs(g - r)[nz] / np.abs(r[nz]))) if nz.any() else 0.0)
+    out["max_rel_err_vs_fp64"] = max(errs)
+    out["rel_tol"] = 1e-6
+    out["pass"] = bool(out["counts_equal"] and out["max_rel_err_vs_fp64"] <= 1e-6)
+    return out
 
 
 # ---------------------------------------------------------------- engine arm
@@ -322,6 +413,9 @@ def engine_arm(args, D):
         d2h = 102 * 24
         launches = 3 * args.steps
         st = {}
+        par = None
+        if D.rank == 0 and D.world == 1 and not args.no_parity:
+            par = brute_parity(eng, pts)
     else:
         cat = T.Catalog(eng, W["los"], W["px"], W["order"])
         for _ in range(args.warmup):
@@ -350,7 +444,9 @@ def engine_arm(args, D):
                        "pair_kernel" if st["num_run_items"] == 0 else "grid/run/pair kernels")
         evaluated = int(st["num_pixel_pairs_evaluated"])
         launches = LAUNCHES_PER_RUN * args.steps
-        jk = None
+        jk = par = None
+        if D.rank == 0 and D.world == 1 and not args.no_parity:
+            par = parity_measure(eng, cat, W, bins)
         if D.rank == 0 and D.world == 1 and not args.no_jackknife:
             jk = jackknife_measure(eng, cat, W, ms_max / args.steps / 1e3, bins)
         cat.close()
@@ -385,9 +481,9 @@ def engine_arm(args, D):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": dict(W["config"], parallelism=f"replicas x{D.world}",
-                           l2_note="catalogue (>1 GB) larger than L2 between steps" if "pts" not in W
-                           else "points fit in L2; all-pairs compute-bound"),
+            "config": W["config"], "parallelism": f"replicas x{D.world}",
+            "l2": ("catalogue (>1 GB) larger than L2 between steps" if "pts" not in W
+                   else "points fit in L2; all-pairs compute-bound"),
             "roofline": roof,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
@@ -400,6 +496,8 @@ def engine_arm(args, D):
         line["grid_sweep_sightline_pairs_per_step"] = int(st["num_grid_items"])
         line["run_sweep_sightline_pairs_per_step"] = int(st["num_run_items"])
         line["ms_expand"] = st["ms_expand"]
+    if par is not None:
+        line["parity"] = par
     if D.rank == 0 and D.world == 1 and "pts" not in W:
         if jk is not None:
             line["jackknife"] = jk
@@ -412,9 +510,9 @@ def engine_arm(args, D):
             line["serving"] = serving_measure(W, args.requests, args.serve_max)
             line["serving"]["section_wall_s"] = time.perf_counter() - t
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
-        v, desc = cpu_sample(W, args.cpu_seconds, os.cpu_count() or 1)
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-                                "sample": desc + "; oracle/xi_oracle.c built with -O3 -ffast-math"}
+        v, kind, desc = cpu_sample(W, os.cpu_count() or 1, args.cpu_cells)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": kind,
+                                "sample": desc}
     if D.rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

@@ -329,7 +329,9 @@ tos_status tos_catalog_device_bytes(const tos_catalog* catalog, uint64_t* bytes)
  * (gpu/brute.cu:40-48).  Outputs have nbins+2 entries:
  *   dsum[k] = sum w_i w_j d_i d_j, wsum[k] = sum w_i w_j, counts[k] = pairs.
  * Binning is exact against the FP64 separation (FP32 fast path with an FP64
- * recheck near bin edges). */
+ * recheck near bin edges).  nbins in [1, 4096]: each warp keeps a
+ * shared-memory window of the nbins + 2 bins, and a block holds as many
+ * warps (up to 16) as the device's shared memory has windows for. */
 tos_status tos_brute_run(tos_engine* engine, const float* points, size_t n_points, double min,
                          double max, int nbins, double* dsum, double* wsum, uint64_t* counts,
                          double* ms_kernel);
@@ -340,15 +342,18 @@ tos_status tos_brute_run(tos_engine* engine, const float* points, size_t n_point
  * cudaMalloc would synchronise the device or is not allowed, loops that must
  * not touch the allocator).  points (n_points x 5 floats: x, y, z, delta, w),
  * dsum, wsum and counts (nbins + 2 each) are DEVICE pointers on the engine's
- * device; results equal tos_brute_run's.  All scratch lives in one static
- * device array of about 12.7 MB that the library reserves on every GPU that
- * loads it, until the process exits, which limits a call to n_points <=
- * 262144 and nbins <= 4096 (larger requests fail with TOS_ERR_INVALID_ARG).
- * The first call on a device looks up that array (and may load the module
- * on the device): make it before any stream capture.  Every call shares the
- * array, so calls that overlap on the GPU (other engines or threads on the
- * same device) race; the call synchronises the engine's stream before it
- * returns. */
+ * device; results equal tos_brute_run's.  The call reads the points and
+ * writes the results on the engine's own stream, with no ordering against
+ * the caller's streams: the writes that produced the points must be complete
+ * (for example the caller's stream synchronised) before the call.  All
+ * scratch lives in one static device array of about 12.7 MB that the
+ * library reserves on every GPU that loads it, until the process exits,
+ * which limits a call to n_points <= 262144 and nbins <= 4096 (larger
+ * requests fail with TOS_ERR_INVALID_ARG).  The first call on a device looks
+ * up that array (and may load the module on the device): make it before any
+ * stream capture.  Every call shares the array, so calls that overlap on the
+ * GPU (other engines or threads on the same device) race; the call
+ * synchronises the engine's stream before it returns. */
 tos_status tos_brute_run_noalloc(tos_engine* engine, const float* points, size_t n_points,
                                  double min, double max, int nbins, double* dsum, double* wsum,
                                  uint64_t* counts, double* ms_kernel);

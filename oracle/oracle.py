@@ -1,10 +1,13 @@
-"""ctypes wrapper of the CPU oracle (oracle/xi_oracle.c).
+"""ctypes wrappers of the CPU oracle (oracle/xi_oracle.c) and of the
+reference's own XiEstimator built from its unchanged sources
+(oracle/ref_harness.cc -> oracle/_ref/libtosref*.so).
 
 TEST INFRASTRUCTURE: used by tests/, __graft_entry__.smoke() and the CPU
-baseline leg of bench.py only, as the checker or the timed reference CPU path.
-The engine never loads it.  Parity unpinned: the reference ships no expected
-outputs for this path and cannot be built here; see the header of
-xi_oracle.c for what the oracle is checked against.
+legs of bench.py only, as the checker or the timed reference CPU path.
+The engine never loads either library.  The oracle is pinned to the
+reference build: tests/golden holds the reference build's outputs for the
+golden catalogues, and tests compare the oracle with them (and with the
+live reference build wherever oracle/_ref has been built).
 """
 from __future__ import annotations
 
@@ -50,6 +53,8 @@ def lib(kind: str = "strict") -> C.CDLL:
         L.orc_cell_costs.restype = C.c_long
         L.orc_brute.argtypes = [vp, sz, dbl, dbl, i32, i32, vp, vp, vp]
         L.orc_brute.restype = C.c_int
+        L.orc_brute_rows.argtypes = [vp, sz, sz, dbl, dbl, i32, i32, vp, vp, vp]
+        L.orc_brute_rows.restype = C.c_int
         L.orc_radec2pix.argtypes = [i32, dbl, dbl]
         L.orc_radec2pix.restype = C.c_int64
         L.orc_bin_pair.argtypes = [i32, vp, dbl, C.c_float, C.c_float, C.c_float, C.c_float, dbl,
@@ -115,6 +120,19 @@ def brute(points, rmin: float, rmax: float, nbins: int, nthreads: int = 0, kind:
     return dsum, wsum, cnt
 
 
+def brute_rows(points, rows: int, rmin: float, rmax: float, nbins: int, nthreads: int = 0, kind: str = "strict"):
+    """Pairs (i, j) with i < rows and i < j: the first rows of the grid against every later row."""
+    L = lib(kind)
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    dsum = np.zeros(nbins + 2)
+    wsum = np.zeros(nbins + 2)
+    cnt = np.zeros(nbins + 2, dtype=np.uint64)
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    L.orc_brute_rows(_p(pts), len(pts), rows, rmin, rmax, nbins, nthreads, _p(dsum), _p(wsum), _p(cnt))
+    return dsum, wsum, cnt
+
+
 def radec2pix(order: int, ra: float, dec: float) -> int:
     return int(lib().orc_radec2pix(order, ra, dec))
 
@@ -125,3 +143,106 @@ def bin_pair(coord: int, axes, scale: float, d1, l1, d2, l2, c):
     out = C.c_uint32()
     ok = lib().orc_bin_pair(coord, _p(axes), scale, d1, l1, d2, l2, c, C.byref(out))
     return int(out.value) if ok else None
+
+
+# ---- the reference's own XiEstimator (oracle/_ref, built by `make -C oracle ref`)
+
+REF_DIR = os.path.join(_HERE, "_ref")
+_ref_libs = {}
+
+
+def ref_available(kind: str = "strict") -> bool:
+    name = {"strict": "libtosref.so", "fast": "libtosref_fast.so", "brute": "libtosref_brute.so"}[kind]
+    return os.path.exists(os.path.join(REF_DIR, name))
+
+
+def ref_lib(kind: str = "strict") -> C.CDLL:
+    """kind: 'strict' (parity pin), 'fast' (the reference's -O3 -ffast-math) or 'brute' (gpu/brute.cu)."""
+    if kind not in _ref_libs:
+        name = {"strict": "libtosref.so", "fast": "libtosref_fast.so", "brute": "libtosref_brute.so"}[kind]
+        path = os.path.join(REF_DIR, name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (make -C oracle ref needs the reference tree)")
+        L = C.CDLL(path)
+        vp, sz, i32, dbl = C.c_void_p, C.c_size_t, C.c_int, C.c_double
+        if kind == "brute":
+            L.tosref_brute.argtypes = [vp, sz, dbl, dbl, i32, C.c_long, vp]
+            L.tosref_brute.restype = C.c_int
+        else:
+            L.tosref_xi.argtypes = [vp, vp, vp, vp, sz, vp, i32, i32, vp, dbl, i32, vp, sz, vp, vp, vp, vp, sz,
+                                    vp, vp, vp, C.c_char_p, sz]
+            L.tosref_xi.restype = C.c_long
+            L.tosref_radec2pix.argtypes = [i32, dbl, dbl]
+            L.tosref_radec2pix.restype = C.c_int64
+            L.tosref_max_centre_distance.argtypes = [i32, vp, sz, C.POINTER(C.c_double)]
+            L.tosref_max_centre_distance.restype = C.c_double
+        _ref_libs[kind] = L
+    return _ref_libs[kind]
+
+
+REF_COUNTERS = ("num_sightline_pairs", "num_sightline_pairs_used", "num_pixels", "num_pixel_pairs",
+                "num_pixel_pairs_used")
+
+
+def ref_xi(sightlines, pixels, order: int, coord: int, axes, scale: float, nthreads: int = 0, cell_subset=None,
+           subsamples: bool = False, kind: str = "strict"):
+    """The reference XiEstimator::run over the catalogue (cell_subset: HEALPix
+    ids of the primary cells to run, default all).  Returns (bins, final,
+    cells or None, cell_ids, stats): raw per-bin totals (the per-cell rows
+    summed in ascending cell order), the finalized xi_, the per-cell rows of
+    the cells run, their ids, and the reference counters plus run_seconds,
+    the wall time of XiEstimator::run alone."""
+    L = ref_lib(kind)
+    ra = np.ascontiguousarray(sightlines["ra"], dtype=np.float64)
+    dec = np.ascontiguousarray(sightlines["dec"], dtype=np.float64)
+    off = np.ascontiguousarray(sightlines["pixel_offset"], dtype=np.uint64)
+    npx = np.ascontiguousarray(sightlines["num_pixels"], dtype=np.uint32)
+    px = np.ascontiguousarray(pixels)
+    axes = np.ascontiguousarray(axes, dtype=np.float64)
+    nb = int(axes[2] * axes[5] * axes[8])
+    sub = None if cell_subset is None else np.ascontiguousarray(cell_subset, dtype=np.int64)
+    cap = len(sub) if sub is not None else len(ra)
+    bins = np.zeros(nb, dtype=XIBIN_DTYPE)
+    final = np.zeros(nb, dtype=XIBIN_DTYPE)
+    cells = np.zeros((cap, nb), dtype=XIBIN_DTYPE) if subsamples else None
+    ids = np.zeros(cap, dtype=np.int64)
+    cnt = np.zeros(5, dtype=np.uint64)
+    ang = np.zeros(2)
+    err = C.create_string_buffer(512)
+    secs = C.c_double()
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    n = L.tosref_xi(_p(ra), _p(dec), _p(off), _p(npx), len(ra), _p(px), order, coord, _p(axes), scale, nthreads,
+                    _p(sub), 0 if sub is None else len(sub), _p(bins), _p(final), _p(cells), _p(ids), cap,
+                    _p(cnt), _p(ang), C.byref(secs), err, 512)
+    if n < 0:
+        raise ValueError("reference XiEstimator failed: " + err.value.decode())
+    st = {k: int(v) for k, v in zip(REF_COUNTERS, cnt)}
+    st["max_ang"], st["cos_max_ang"] = float(ang[0]), float(ang[1])
+    st["run_seconds"] = secs.value
+    return bins, final, (cells[:n] if cells is not None else None), ids[:n], st
+
+
+def ref_radec2pix(order: int, ra: float, dec: float) -> int:
+    return int(ref_lib().tosref_radec2pix(order, ra, dec))
+
+
+def ref_max_centre_distance(order: int, dirs):
+    """(largest direction-to-own-pixel-centre distance over dirs, the bound
+    the stand-in query_disc_inclusive adds to the radius)."""
+    d = np.ascontiguousarray(dirs, dtype=np.float64)
+    bound = C.c_double()
+    worst = ref_lib().tosref_max_centre_distance(order, _p(d), len(d), C.byref(bound))
+    return float(worst), float(bound.value)
+
+
+def ref_brute_gpu(points, rmin: float, rmax: float, nbins: int, chunksize: int = 4096):
+    """The reference's bruteGPU (gpu/brute.cu:63-225) on the GPU: xi per bin
+    (FP32 histograms).  Needs a CUDA device."""
+    L = ref_lib("brute")
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    xi = np.zeros(nbins)
+    r = L.tosref_brute(_p(pts), len(pts), rmin, rmax, nbins, chunksize, _p(xi))
+    if r < 0:
+        raise ValueError("reference bruteGPU rejected the input")
+    return xi

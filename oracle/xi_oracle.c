@@ -455,7 +455,7 @@ long orc_cell_costs(const double* ra, const double* dec, const uint32_t* npix, s
 /* ---------------- brute-force estimator ------------------------------------ */
 typedef struct {
   const float* p;
-  size_t n;
+  size_t n, rows; /* pairs (i, j) with i < rows and i < j < n */
   double min, max, spacing;
   int nbins;
   double* dsum; double* wsum; uint64_t* cnt; /* per thread [nbins+2] */
@@ -470,7 +470,7 @@ static void* brute_worker(void* arg) {
   double* ds = J->dsum + (size_t)A->t * nb;
   double* ws = J->wsum + (size_t)A->t * nb;
   uint64_t* ct = J->cnt + (size_t)A->t * nb;
-  for (size_t i = (size_t)A->t; i < J->n; i += (size_t)J->nthreads) {
+  for (size_t i = (size_t)A->t; i < J->rows; i += (size_t)J->nthreads) {
     const float* a = J->p + 5 * i;
     const double wdi = (double)a[4] * (double)a[3], wi = a[4];
     for (size_t j = i + 1; j < J->n; ++j) {
@@ -494,13 +494,14 @@ static void* brute_worker(void* arg) {
   return NULL;
 }
 
-/* All pairs i < j of n points (x,y,z,delta,w rows); outputs nbins+2 entries. */
-int orc_brute(const float* points, size_t n, double min, double max, int nbins, int nthreads,
-              double* dsum, double* wsum, uint64_t* counts) {
+/* Pairs (i, j), i < rows and i < j < n, of n points (x,y,z,delta,w rows);
+ * outputs nbins+2 entries.  rows = n gives all pairs. */
+int orc_brute_rows(const float* points, size_t n, size_t rows, double min, double max, int nbins, int nthreads,
+                   double* dsum, double* wsum, uint64_t* counts) {
   if (nthreads < 1) nthreads = 1;
   const int nb = nbins + 2;
   orc_brute_job J;
-  J.p = points; J.n = n; J.min = min; J.max = max; J.spacing = (max - min) / nbins; J.nbins = nbins;
+  J.p = points; J.n = n; J.rows = rows < n ? rows : n; J.min = min; J.max = max; J.spacing = (max - min) / nbins; J.nbins = nbins;
   J.nthreads = nthreads;
   J.dsum = (double*)calloc((size_t)nthreads * nb, 8);
   J.wsum = (double*)calloc((size_t)nthreads * nb, 8);
@@ -518,6 +519,12 @@ int orc_brute(const float* points, size_t n, double min, double max, int nbins, 
     }
   free(J.dsum); free(J.wsum); free(J.cnt); free(th); free(args);
   return 0;
+}
+
+/* All pairs i < j of n points. */
+int orc_brute(const float* points, size_t n, double min, double max, int nbins, int nthreads,
+              double* dsum, double* wsum, uint64_t* counts) {
+  return orc_brute_rows(points, n, n, min, max, nbins, nthreads, dsum, wsum, counts);
 }
 
 /* Exact single-pair binning, for tests of the expression order. Returns 1

@@ -46,6 +46,46 @@ def test_brute_random_points(engine):
     assert np.max(np.abs(ds[nzd] - ods[nzd]) / np.abs(ods[nzd])) < 1e-6
 
 
+@pytest.mark.parametrize("nbins", [603, 604, 1000, 4096])
+def test_brute_many_bins(engine, nbins):
+    """Bin counts whose shared-memory windows do not fit 16 warps per block
+    (above 603 bins the block holds fewer warps), up to the 4096 limit."""
+    pts = grid_points(12, 5.0, seed=nbins, weights=True)
+    ds, ws, ct, _ = T.brute_run(engine, pts, 0.0, 90.0, nbins)
+    ods, ows, oct_ = oracle.brute(pts, 0.0, 90.0, nbins)
+    assert np.array_equal(ct, oct_), np.nonzero(ct != oct_)[0][:10]
+    nz = ows != 0
+    assert np.max(np.abs(ws[nz] - ows[nz]) / np.abs(ows[nz])) < 1e-9
+    nzd = ods != 0
+    assert np.max(np.abs(ds[nzd] - ods[nzd]) / np.abs(ods[nzd])) < 1e-6
+
+
+def test_brute_rejects_too_many_bins(engine):
+    pts = grid_points(4, 5.0, seed=1)
+    with pytest.raises(T.TosError) as e:
+        T.brute_run(engine, pts, 0.0, 90.0, 4097)
+    assert e.value.status == 1
+
+
+def test_brute_full_config_rows_vs_oracle(engine):
+    """The 64^3 benchmark grid: pairs (i, j) with i < 256 and j > i, the
+    difference of the engine's all-pairs counts over the grid and over its
+    rows [256, n), against the FP64 oracle bin by bin."""
+    pts = T.synth.grf_grid(64, 256.0, seed=3)
+    m = 256
+    full = T.brute_run(engine, pts, 0.0, 200.0, 100)
+    tail = T.brute_run(engine, pts[m:], 0.0, 200.0, 100)
+    ods, ows, oct_ = oracle.brute_rows(pts, m, 0.0, 200.0, 100)
+    ct = full[2].astype(np.int64) - tail[2].astype(np.int64)
+    assert np.array_equal(ct, oct_.astype(np.int64))
+    assert int(oct_.sum()) == sum(len(pts) - 1 - i for i in range(m))
+    ws = full[1] - tail[1]
+    np.testing.assert_array_equal(ws, ows)  # w = 1: weight sums are counts
+    ds = full[0] - tail[0]
+    nzd = ods != 0
+    assert np.max(np.abs(ds[nzd] - ods[nzd]) / np.abs(ods[nzd])) < 1e-6
+
+
 def test_brute_full_config_invariants(engine):
     pts = T.synth.grf_grid(64, 256.0, seed=3)
     ds, ws, ct, ms = T.brute_run(engine, pts, 0.0, 200.0, 100)

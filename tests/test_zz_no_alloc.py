@@ -57,6 +57,12 @@ def test_noalloc_matches_allocating_entry_point_twice(engine):
     check_same(run_noalloc(engine, b, 5.0, 80.0, 17), T.brute_run(engine, b, 5.0, 80.0, 17))
 
 
+def test_noalloc_at_the_bin_limit(engine):
+    pytest.importorskip("torch")
+    a = make_points(3000, seed=3)
+    check_same(run_noalloc(engine, a, 0.0, 100.0, 4096), T.brute_run(engine, a, 0.0, 100.0, 4096))
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch(engine):
     with pytest.raises(T.TosError) as e:
         T.brute_run_noalloc(engine, 1, (1 << 18) + 1, 0.0, 100.0, 10, 1, 1, 1)

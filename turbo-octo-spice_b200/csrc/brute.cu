@@ -218,6 +218,20 @@ __global__ void __launch_bounds__(kBruteWarps * 32, 1) brute_kernel(BruteArgs A)
   if (lane == 0) atomicAdd(&A.counters[0], n_recheck);
 }
 
+// Launch shape: a warp's window holds kBWords words for each of the
+// nbins + 2 bins, so as many warps (up to kBruteWarps) as the block's opt-in
+// shared memory holds windows for.  The kernel takes its warp count from the
+// block size.  Fails only if not even one window fits.
+tos_status brute_shape(const tos_engine* e, int nbins, int* warps, size_t* smem) {
+  const size_t per_warp = (size_t)kBWords * (nbins + 2) * sizeof(uint32_t);
+  const size_t fit = e->smem_optin / per_warp;
+  if (fit < 1)
+    return fail(TOS_ERR_UNSUPPORTED, "nbins too large for one warp's shared-memory window on this device");
+  *warps = (int)std::min<size_t>(kBruteWarps, fit);
+  *smem = (size_t)*warps * per_warp;
+  return TOS_OK;
+}
+
 __global__ void k_brute_prep(const float* pts, int n, float4* pos, double* wd, double* w) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const float* p = pts + 5 * (size_t)k;
@@ -340,11 +354,13 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
   A.counts = d_counts.p;
   A.next = d_misc.p;
   A.counters = d_misc.p + 1;
-  const size_t smem = (size_t)kBruteWarps * kBWords * (nbins + 2) * sizeof(uint32_t);
+  int warps = 0;
+  size_t smem = 0;
+  TOS_TRY(brute_shape(e, nbins, &warps, &smem));
   TOS_CUDA_TRY(cudaFuncSetAttribute(brute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
-  brute_kernel<<<e->num_sms, kBruteWarps * 32, smem, st>>>(A);
+  brute_kernel<<<e->num_sms, warps * 32, smem, st>>>(A);
   TOS_CUDA_TRY(cudaGetLastError());
   TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
   std::vector<double> out((size_t)(nbins + 2) * 2);
@@ -370,9 +386,8 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
 //
 // Some callers cannot allocate device memory while they count pairs: code
 // that manages every byte of the GPU through its own pool, code that runs
-// where a cudaMalloc would synchronise the device or is not allowed (for
-// instance between the start and end of a stream capture), or service loops
-// that must not touch the allocator at all.  tos_brute_run allocates its
+// where a cudaMalloc would synchronise the device or is not allowed, or
+// service loops that must not touch the allocator at all.  tos_brute_run allocates its
 // scratch on every call; tos_brute_run_noalloc takes its inputs and outputs
 // in device memory and keeps all scratch in one statically sized device
 // array that the library reserves on every GPU that loads it, until exit.
@@ -538,11 +553,13 @@ extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points
   A.counts = cnt;
   A.next = misc;
   A.counters = misc + 1;
-  const size_t smem = (size_t)kBruteWarps * kBWords * nb2 * sizeof(uint32_t);
+  int warps = 0;
+  size_t smem = 0;
+  TOS_TRY(brute_shape(e, nbins, &warps, &smem));
   TOS_CUDA_TRY(cudaFuncSetAttribute(brute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
-  brute_kernel<<<e->num_sms, kBruteWarps * 32, smem, st>>>(A);
+  brute_kernel<<<e->num_sms, warps * 32, smem, st>>>(A);
   TOS_CUDA_TRY(cudaGetLastError());
   TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
   k_brute_unpack<<<(nb2 + 255) / 256, 256, 0, st>>>(out, cnt, nb2, d_dsum, d_wsum, d_counts);

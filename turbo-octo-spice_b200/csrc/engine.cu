@@ -606,6 +606,7 @@ tos_status tos_engine_create(int device, tos_engine** out) {
   auto* e = new tos_engine();
   e->device = device;
   e->num_sms = prop.multiProcessorCount;
+  e->smem_optin = prop.sharedMemPerBlockOptin;
   DeviceGuard g(device);
   if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete e;

@@ -95,6 +95,7 @@ struct Workspace {
 struct tos_engine {
   int device = 0;
   int num_sms = 0;
+  size_t smem_optin = 0;  // opt-in shared memory per block (bytes)
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[7] = {};
   std::mutex mu;

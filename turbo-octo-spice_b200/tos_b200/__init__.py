@@ -183,6 +183,12 @@ class Grid:
     def observing(dloglam="[0:0.05]*25", theta="[5:175]*1", z="[3.556:3.735]*1") -> "Grid":
         return Grid(OBSERVING, tuple(Axis.parse(a) for a in (dloglam, theta, z)))
 
+    @staticmethod
+    def from_axes(coord_type: int, axes) -> "Grid":
+        """Grid of a coordinate type from nine values (min, max, nbins) x 3."""
+        a = np.asarray(axes, dtype=np.float64).reshape(3, 3)
+        return Grid(int(coord_type), tuple(Axis(float(x[0]), float(x[1]), int(x[2])) for x in a))
+
     def c_struct(self) -> _Grid:
         g = _Grid()
         g.type = self.type
