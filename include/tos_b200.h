@@ -120,6 +120,8 @@ typedef struct {
   double ms_runs;                    /* device time: grid- and run-sweep kernels (part of ms_pairs) */
   uint64_t num_grid_items;           /* of num_run_items: sightline pairs counted by the grid-sweep kernel */
   double ms_grid;                    /* device time: grid-sweep kernel (part of ms_runs) */
+  uint64_t num_diag_items;           /* sightline pairs counted by the diagonal-sweep kernel (Polar) */
+  double ms_diag;                    /* device time: diagonal-sweep kernel (part of ms_pairs) */
 } tos_xi_stats;
 
 /* Opaque handles. */
@@ -329,12 +331,25 @@ tos_status tos_catalog_device_bytes(const tos_catalog* catalog, uint64_t* bytes)
  * (gpu/brute.cu:40-48).  Outputs have nbins+2 entries:
  *   dsum[k] = sum w_i w_j d_i d_j, wsum[k] = sum w_i w_j, counts[k] = pairs.
  * Binning is exact against the FP64 separation (FP32 fast path with an FP64
- * recheck near bin edges).  nbins in [1, 4096]: each warp keeps a
- * shared-memory window of the nbins + 2 bins, and a block holds as many
- * warps (up to 16) as the device's shared memory has windows for. */
+ * recheck near bin edges); the sums are exact fixed-point sums of FP64
+ * products, the same for every launch shape.  2 <= n_points <= 2^24 and
+ * nbins in [1, 4096]: each warp keeps a shared-memory window of the nbins + 2
+ * bins, and a block holds as many warps (up to 16) as the device's shared
+ * memory has windows for. */
 tos_status tos_brute_run(tos_engine* engine, const float* points, size_t n_points, double min,
                          double max, int nbins, double* dsum, double* wsum, uint64_t* counts,
                          double* ms_kernel);
+
+/* Autotuner of tos_brute_run's launch shape for one bin count (the
+ * reference fixes its shape from device properties, gpu/brute.cu:99-131):
+ * times every kernel variant (1, 2 or 4 diagonals per lane) with 4, 8 and 16
+ * warps per CTA on the first min(n_points, 131072) points and keeps the
+ * fastest on the engine.  Later tos_brute_run and tos_brute_run_noalloc calls
+ * with that bin count use it; results do not depend on the shape (exact
+ * integer sums).  The pick is written to *diagonals_per_lane and
+ * *warps_per_cta (either may be null). */
+tos_status tos_brute_tune(tos_engine* engine, const float* points, size_t n_points, double min,
+                          double max, int nbins, int* diagonals_per_lane, int* warps_per_cta);
 
 /* tos_brute_run without any device allocation.  No counterpart in the
  * reference: it is for callers that cannot allocate GPU memory while they
@@ -346,7 +361,7 @@ tos_status tos_brute_run(tos_engine* engine, const float* points, size_t n_point
  * writes the results on the engine's own stream, with no ordering against
  * the caller's streams: the writes that produced the points must be complete
  * (for example the caller's stream synchronised) before the call.  All
- * scratch lives in one static device array of about 12.7 MB that the
+ * scratch lives in one static device array of about 8.5 MB that the
  * library reserves on every GPU that loads it, until the process exits,
  * which limits a call to n_points <= 262144 and nbins <= 4096 (larger
  * requests fail with TOS_ERR_INVALID_ARG).  The first call on a device looks

@@ -46,10 +46,11 @@ def test_brute_random_points(engine):
     assert np.max(np.abs(ds[nzd] - ods[nzd]) / np.abs(ods[nzd])) < 1e-6
 
 
-@pytest.mark.parametrize("nbins", [603, 604, 1000, 4096])
+@pytest.mark.parametrize("nbins", [322, 323, 686, 687, 1000, 4096])
 def test_brute_many_bins(engine, nbins):
-    """Bin counts whose shared-memory windows do not fit 16 warps per block
-    (above 603 bins the block holds fewer warps), up to the 4096 limit."""
+    """Bin counts whose shared-memory windows do not fit the default 8 warps
+    per block (above 686 bins the block holds fewer warps; above 322, fewer
+    than 16), up to the 4096 limit, where a block holds one warp."""
     pts = grid_points(12, 5.0, seed=nbins, weights=True)
     ds, ws, ct, _ = T.brute_run(engine, pts, 0.0, 90.0, nbins)
     ods, ows, oct_ = oracle.brute(pts, 0.0, 90.0, nbins)
@@ -93,3 +94,18 @@ def test_brute_full_config_invariants(engine):
     assert int(ct.sum()) == n * (n - 1) // 2
     np.testing.assert_allclose(ws, ct.astype(np.float64), rtol=0, atol=0)  # w = 1: sum of weights = count
     assert ct[0] == 0  # no pair below r = 0
+
+
+def test_brute_tune_pick_gives_identical_results(engine):
+    """The autotuner times every launch shape on the points and keeps the
+    fastest for this bin count; counts and sums are exact integer sums, so the
+    tuned shape gives the same results bit for bit."""
+    pts = T.synth.grf_grid(24, 96.0, seed=9)
+    before = T.brute_run(engine, pts, 0.0, 80.0, 40)
+    k, w = T.brute_tune(engine, pts, 0.0, 80.0, 40)
+    assert k in (1, 2, 4) and w in (4, 8, 16)
+    after = T.brute_run(engine, pts, 0.0, 80.0, 40)
+    for a, b in zip(before[:3], after[:3]):
+        assert np.array_equal(a, b)
+    ods, ows, oct_ = oracle.brute(pts, 0.0, 80.0, 40)
+    assert np.array_equal(after[2], oct_)

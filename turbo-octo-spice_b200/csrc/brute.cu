@@ -5,15 +5,23 @@
 // Differences from the reference design, all in service of exactness and
 // throughput:
 //  - points stay resident in HBM (no per-chunk host copies, brute.cu:155-193);
-//  - every unordered pair i < j is visited once by a persistent sweep: a warp
-//    owns 32 consecutive points i (lane = i) and walks j = t + lane, so on a
-//    regular grid every lane has the same separation vector at the same step;
+//  - every unordered pair i < j is visited once, along diagonals: a pair
+//    (i, i + delta) lies on diagonal delta, a lane owns K consecutive
+//    diagonals of a group of 32 K and walks them row by row (i = 0, 1, ...),
+//    so the row's point is a broadcast load and the lane's K columns are a
+//    register window that slides by one column per row.  For points on a
+//    regular grid the separation vector of a diagonal stays the same along
+//    whole runs of rows (until the column wraps to the next grid line), so
+//    the bin of a diagonal changes only every few tens of rows;
 //  - separations are binned in FP32 with an FP64 re-binning of pairs within
 //    2^-K bins of an edge, so bins equal those of the FP64 separation
 //    sqrt(dx^2+dy^2+dz^2) (the double-precision estimator of bucketxi.cc:79-98);
-//  - sums are exact: runs of equal bins are summed from FP64 prefix sums,
-//    quantised to fixed point and added with u32 shared atomics into a
-//    per-warp window, which is added to FP64 global sums when a slot fills.
+//  - sums are exact: while a diagonal stays in one bin the lane adds the
+//    FP64 products w_i d_i w_j d_j and w_i w_j in registers; a run that ends
+//    goes, rounded once to fixed point, into a per-warp shared-memory window
+//    of 128-bit carry-free sums, which is added to the global sums after each
+//    diagonal group.  Integer sums do not depend on the order of the adds, so
+//    the result is the same for every launch shape.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,23 +31,21 @@
 #include <vector>
 
 #include "engine_internal.h"
+#include "fixed128.cuh"
 
 namespace tos {
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr int kBruteWarps = 16;
-constexpr int kBWords = 6;          // dsum lo/hi, wsum lo/hi, count, contributions
-constexpr int kBSplit = 20;
-constexpr uint32_t kSlotLimit = 3800;  // contributions per slot before the window is emptied
-constexpr int kRunCap = 64;            // longest run summed as one contribution
-constexpr double kMagic = 6755399441055744.0;
+constexpr int kBruteWarpsMax = 16;  // warps per CTA at most
+constexpr int kBWin = 5;            // u64 words per bin of a window: dsum lo, hi, wsum lo, hi, count
+constexpr int kBQueue = 64;         // closed runs a warp holds before it adds 32 of them
+constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
 constexpr long long kMagicBits = 0x4338000000000000LL;
 
 struct BruteArgs {
   const float4* pos;      // (x, y, z, 0), n entries
-  const double2* prefix;  // n+1 exclusive prefix sums of (w*delta, w)
-  const double* wd;       // w*delta per point
+  const double* wd;       // w*delta per point (exact product of the two floats)
   const double* w;        // w per point
   int n;
   int nbins;
@@ -48,12 +54,16 @@ struct BruteArgs {
   int k;
   float mag;
   int bits;
-  double scale[2];
-  double inv_scale[2];
-  double* out;            // [nbins+2][2] FP64 sums
-  unsigned long long* counts;  // [nbins+2]
-  unsigned long long* next;    // chunk counter
-  unsigned long long* counters;  // [0] rechecks
+  double scale_hi[2];     // 2^(F - 44) of fields dsum, wsum: |run sum| * 2^F < 2^62
+  unsigned long long* acc;       // [nbins + 2][kBWin] 128-bit carry-free sums and counts
+  unsigned long long* next;      // diagonal-group counter
+  unsigned long long* counters;  // [0] FP64 re-binnings
+};
+
+// A run that ended: bin, pairs and its two FP64 sums.
+struct BRun {
+  uint32_t bin, m;
+  double dsum, wsum;
 };
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -62,8 +72,14 @@ __device__ __forceinline__ float sqrt_approx(float x) {
   return r;
 }
 
-__device__ __forceinline__ long long to_fixed(double c, double scale) {
-  return __double_as_longlong(__fma_rn(c, scale, kMagic)) - kMagicBits;
+// round(c * 2^F) for |c * 2^F| < 2^62, given sh = 2^(F-44): the high part is
+// rounded first and the exact remainder carries the low 44 bits.
+__device__ __forceinline__ long long fixed_wide(double c, double sh) {
+  const double v = c * sh;
+  const long long qh = __double_as_longlong(__dadd_rn(v, kMagic)) - kMagicBits;
+  const double rem = v - (double)qh;  // exact, |rem| <= 0.5
+  const long long ql = __double_as_longlong(__fma_rn(rem, 17592186044416.0 /* 2^44 */, kMagic)) - kMagicBits;
+  return (qh << 44) + ql;
 }
 
 // Histogram index of the FP64 separation: 0 below min, nbins+1 at or above
@@ -79,157 +95,165 @@ __device__ __forceinline__ uint32_t exact_index(const BruteArgs& A, float4 a, fl
   return (uint32_t)k + 1u;
 }
 
-__device__ void flush(const BruteArgs& A, uint32_t* win, int lane) {
-  const int S = A.nbins + 2;
-  for (int s = lane; s < S; s += 32) {
-    const uint32_t cnt = win[4 * S + s];
-    if (cnt == 0) continue;
+// Add the queued runs [first, first + cnt) to the warp window, one per lane.
+__device__ __forceinline__ void brute_drain(const BruteArgs& A, unsigned long long* win, int S,
+                                            const BRun* q, int first, int cnt, int lane) {
+  __syncwarp();
+  if (lane < cnt) {
+    const BRun r = q[first + lane];
+    const long long v0 = fixed_wide(r.dsum, A.scale_hi[0]);
+    const long long v1 = fixed_wide(r.wsum, A.scale_hi[1]);
+    atomicAdd(&win[0 * S + r.bin], (unsigned long long)v0 & 0xFFFFFFFFull);
+    atomicAdd(&win[1 * S + r.bin], (unsigned long long)(v0 >> 32));
+    atomicAdd(&win[2 * S + r.bin], (unsigned long long)v1 & 0xFFFFFFFFull);
+    atomicAdd(&win[3 * S + r.bin], (unsigned long long)(v1 >> 32));
+    atomicAdd(&win[4 * S + r.bin], (unsigned long long)r.m);
+  }
+  __syncwarp();
+}
+
+// Add the warp window to the global sums (carry-free: low 32 bits and the
+// signed rest of each 128-bit window value) and clear it.
+__device__ __forceinline__ void brute_flush(const BruteArgs& A, unsigned long long* win, int S, int lane) {
+  __syncwarp();
+  for (int b = lane; b < S; b += 32) {
+    const unsigned long long cnt = win[4 * S + b];
+    if (cnt == 0) continue;  // every run has at least one pair
+    unsigned long long* g = A.acc + (size_t)b * kBWin;
 #pragma unroll
     for (int f = 0; f < 2; ++f) {
-      const uint32_t lo = win[(2 * f) * S + s];
-      const int hi = (int)win[(2 * f + 1) * S + s];
-      const long long q = ((long long)hi << kBSplit) + (long long)lo;
-      atomicAdd(&A.out[2 * s + f], (double)q * A.inv_scale[f]);
+      const __int128 v = (__int128)(long long)win[(2 * f + 1) * S + b] * (__int128)4294967296ll +
+                         (__int128)win[2 * f * S + b];
+      atomicAdd(&g[2 * f], (unsigned long long)v & 0xFFFFFFFFull);
+      const long long h = (long long)(v >> 32);
+      if (h != 0) atomicAdd(&g[2 * f + 1], (unsigned long long)h);
+      win[2 * f * S + b] = 0ull;
+      win[(2 * f + 1) * S + b] = 0ull;
     }
-    atomicAdd(&A.counts[s], (unsigned long long)cnt);
-#pragma unroll
-    for (int w = 0; w < kBWords; ++w) win[w * S + s] = 0u;
+    atomicAdd(&g[4], cnt);
+    win[4 * S + b] = 0ull;
   }
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kBruteWarps * 32, 1) brute_kernel(BruteArgs A) {
-  extern __shared__ uint32_t smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// Diagonal groups: group g holds diagonals 1 + g * 32K .. 1 + (g + 1) * 32K - 1;
+// lane L owns 1 + g * 32K + K L + m, m = 0 .. K-1.  Longest diagonals first.
+template <int K>
+__global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A) {
+  extern __shared__ unsigned long long bsm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int S = A.nbins + 2;
-  uint32_t* win = smem + (size_t)warp * kBWords * S;
-  for (int k = lane; k < kBWords * S; k += 32) win[k] = 0u;
+  unsigned long long* win = bsm + (size_t)warp * kBWin * S;
+  BRun* q = reinterpret_cast<BRun*>(bsm + (size_t)nw * kBWin * S) + warp * kBQueue;
+  for (int k = lane; k < kBWin * S; k += 32) win[k] = 0ull;
   __syncwarp();
+  const unsigned lt = (1u << lane) - 1u;
+  const int span = 32 * K;
+  const long long ngroups = ((long long)A.n - 1 + span - 1) / span;
   unsigned long long n_recheck = 0;
-  const int nchunks = (A.n + 31) / 32;
-  bool full = false;
   for (;;) {
-    unsigned long long c = 0;
-    if (lane == 0) c = atomicAdd(A.next, 1ull);
-    c = __shfl_sync(kFull, c, 0);
-    if (c >= (unsigned long long)nchunks) break;
-    // big chunks (long sweeps) first: chunk c covers rows i0 = 32*c'
-    const int i0 = 32 * (int)c;
-    const int i = i0 + lane;
-    const bool active = i < A.n;
-    const float4 pi = active ? A.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const double wdi = active ? A.wd[i] : 0.0, wi = active ? A.w[i] : 0.0;
-    uint32_t cur = 0xFFFFFFFFu;
-    int run_start = 0;
-    double ps0 = 0, ps1 = 0;
-    // Add the runs that lanes with `emit` close (bin `slot`, its words):
-    // lanes closing a run in the same bin, which on a regular grid is most
-    // of the warp (one separation vector per step), sum their words with
-    // redux.sync and one of them adds the sums to the window.
-    auto emit_runs = [&](bool emit, uint32_t slot, const uint32_t (&wv)[5]) {
-      unsigned pending = __ballot_sync(kFull, emit);
-      while (pending) {
-        const int leader = __ffs(pending) - 1;
-        const uint32_t ls = __shfl_sync(kFull, slot, leader);
-        const unsigned peers = __ballot_sync(kFull, ((pending >> lane) & 1u) && slot == ls);
-        if ((peers >> lane) & 1u) {
-          uint32_t sw[5];
+    unsigned long long g = 0;
+    if (lane == 0) g = atomicAdd(A.next, 1ull);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= (unsigned long long)ngroups) break;
+    const int dg = 1 + (int)g * span;  // the group's first diagonal
+    const int d0 = dg + K * lane;      // this lane's first diagonal
+    const int t_end = A.n - dg;        // rows with a pair on the group's first diagonal
+    uint32_t cur[K];
+    int s0[K];
+    double ds[K], ws[K];
+    float4 cp[K];
+    double cwd[K], cw[K];
 #pragma unroll
-          for (int w = 0; w < 5; ++w) sw[w] = __reduce_add_sync(peers, wv[w]);
-          if (lane == leader) {
+    for (int m = 0; m < K; ++m) {
+      cur[m] = 0xFFFFFFFFu;
+      s0[m] = 0;
+      ds[m] = ws[m] = 0.0;
+    }
+    // columns of row 0: d0 + m (the newest, m = K - 1, is loaded in the loop)
 #pragma unroll
-            for (int w = 0; w < 5; ++w) atomicAdd(&win[w * S + ls], sw[w]);
-            const uint32_t n = (uint32_t)__popc(peers);
-            const uint32_t old = atomicAdd(&win[5 * S + ls], n);
-            if (old + n > kSlotLimit) full = true;
-          }
-        }
-        pending &= ~peers;
+    for (int m = 0; m + 1 < K; ++m) {
+      const int jc = min(d0 + m, A.n - 1);
+      cp[m] = A.pos[jc];
+      cwd[m] = A.wd[jc];
+      cw[m] = A.w[jc];
+    }
+    int qn = 0;  // queued runs (the same in every lane)
+#pragma unroll 1
+    for (int t = 0; t < t_end; ++t) {
+      {
+        const int jc = min(t + d0 + K - 1, A.n - 1);
+        cp[K - 1] = A.pos[jc];
+        cwd[K - 1] = A.wd[jc];
+        cw[K - 1] = A.w[jc];
       }
-    };
-    auto run_words = [&](int p_end, double2 pn, uint32_t (&wv)[5]) {
-      const double c0 = wdi * (pn.x - ps0), c1 = wi * (pn.y - ps1);
-      const long long q0 = to_fixed(c0, A.scale[0]), q1 = to_fixed(c1, A.scale[1]);
-      wv[0] = (uint32_t)q0 & ((1u << kBSplit) - 1u);
-      wv[1] = (uint32_t)(int)(q0 >> kBSplit);
-      wv[2] = (uint32_t)q1 & ((1u << kBSplit) - 1u);
-      wv[3] = (uint32_t)(int)(q1 >> kBSplit);
-      wv[4] = (uint32_t)(p_end - run_start);
-    };
-    for (int t = i0 + 1; t < A.n; ++t) {
-      const int j = t + lane;
-      uint32_t key = 0xFFFFFFFFu;
-      bool recheck = false;
-      float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (active && j < A.n) {
-        pj = A.pos[j];
-        const float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y),
-                    dz = __fsub_rn(pi.z, pj.z);
+      const float4 pi = A.pos[t];
+      const double wdi = A.wd[t], wi = A.w[t];
+#pragma unroll
+      for (int m = 0; m < K; ++m) {
+        const bool in = t + d0 + m < A.n;
+        const float dx = __fsub_rn(pi.x, cp[m].x), dy = __fsub_rn(pi.y, cp[m].y),
+                    dz = __fsub_rn(pi.z, cp[m].z);
         const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
         const float tt = __fmaf_rn(sqrt_approx(r2), A.invf, A.offf);
-        const int q = __float_as_int(__fadd_rz(tt, A.mag)) - A.bits;
-        int b = (q >> A.k) + 1;
+        const int qq = __float_as_int(__fadd_rz(tt, A.mag)) - A.bits;
+        int b = (qq >> A.k) + 1;
         b = (tt < 0.f) ? 0 : ((tt >= A.nbf) ? A.nbins + 1 : b);
-        key = (uint32_t)b;
-        recheck = (((q + 1) & ((1 << A.k) - 1)) < 2) && (tt < A.nbp1f) && (tt > -1.f);
-      }
-      if (__any_sync(kFull, recheck)) {
-        if (recheck) {
-          key = exact_index(A, pi, pj);
-          ++n_recheck;
+        uint32_t key = in ? (uint32_t)b : 0xFFFFFFFFu;
+        const bool recheck = in && (((qq + 1) & ((1 << A.k) - 1)) < 2) && (tt < A.nbp1f) && (tt > -1.f);
+        if (__any_sync(kFull, recheck)) {
+          if (recheck) {
+            key = exact_index(A, pi, cp[m]);
+            ++n_recheck;
+          }
         }
-      }
-      const bool change = (key != cur) || (cur != 0xFFFFFFFFu && j - run_start >= kRunCap);
-      if (__any_sync(kFull, change)) {
-        uint32_t wv[5] = {0u, 0u, 0u, 0u, 0u};
-        const bool emit = change && cur != 0xFFFFFFFFu;
-        const uint32_t slot = cur;
+        const bool change = key != cur[m];
+        const bool close = change && cur[m] != 0xFFFFFFFFu;
+        const unsigned cm = __ballot_sync(kFull, close);
+        if (cm) {
+          if (close) q[qn + __popc(cm & lt)] = BRun{cur[m], (uint32_t)(t - s0[m]), ds[m], ws[m]};
+          qn += __popc(cm);
+          if (qn >= 32) {
+            qn -= 32;
+            brute_drain(A, win, S, q, qn, 32, lane);
+          }
+        }
         if (change) {
-          const int pc = min(j, A.n);
-          const double2 pn = A.prefix[pc];
-          if (emit) run_words(j, pn, wv);
-          cur = key;
-          run_start = j;
-          ps0 = pn.x;
-          ps1 = pn.y;
+          cur[m] = key;
+          s0[m] = t;
+          ds[m] = 0.0;
+          ws[m] = 0.0;
         }
-        emit_runs(emit, slot, wv);
-        if (__any_sync(kFull, full)) {
-          flush(A, win, lane);
-          full = false;
+        if (in) {
+          ds[m] = __fma_rn(wdi, cwd[m], ds[m]);
+          ws[m] = __fma_rn(wi, cw[m], ws[m]);
         }
       }
+#pragma unroll
+      for (int m = 0; m + 1 < K; ++m) {
+        cp[m] = cp[m + 1];
+        cwd[m] = cwd[m + 1];
+        cw[m] = cw[m + 1];
+      }
     }
-    {
-      // the sweep ended at t = n-1, so lane's last j = n-1+lane; runs only
-      // cover real points, hence every open run ends at n
-      uint32_t wv[5] = {0u, 0u, 0u, 0u, 0u};
-      const bool emit = cur != 0xFFFFFFFFu;
-      if (emit) run_words(A.n, A.prefix[A.n], wv);
-      emit_runs(emit, cur, wv);
+    // runs still open: a diagonal's last pair is at row n - 1 - delta, and
+    // every row after it was out of range, which already closed the run
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+      const bool close = cur[m] != 0xFFFFFFFFu;
+      const unsigned cm = __ballot_sync(kFull, close);
+      if (close) q[qn + __popc(cm & lt)] = BRun{cur[m], (uint32_t)(t_end - s0[m]), ds[m], ws[m]};
+      qn += __popc(cm);
+      if (qn >= 32) {
+        qn -= 32;
+        brute_drain(A, win, S, q, qn, 32, lane);
+      }
     }
-    if (__any_sync(kFull, full)) {
-      flush(A, win, lane);
-      full = false;
-    }
+    brute_drain(A, win, S, q, 0, qn, lane);
+    brute_flush(A, win, S, lane);
   }
-  flush(A, win, lane);
   for (int o = 16; o > 0; o >>= 1) n_recheck += __shfl_xor_sync(kFull, n_recheck, o);
   if (lane == 0) atomicAdd(&A.counters[0], n_recheck);
-}
-
-// Launch shape: a warp's window holds kBWords words for each of the
-// nbins + 2 bins, so as many warps (up to kBruteWarps) as the block's opt-in
-// shared memory holds windows for.  The kernel takes its warp count from the
-// block size.  Fails only if not even one window fits.
-tos_status brute_shape(const tos_engine* e, int nbins, int* warps, size_t* smem) {
-  const size_t per_warp = (size_t)kBWords * (nbins + 2) * sizeof(uint32_t);
-  const size_t fit = e->smem_optin / per_warp;
-  if (fit < 1)
-    return fail(TOS_ERR_UNSUPPORTED, "nbins too large for one warp's shared-memory window on this device");
-  *warps = (int)std::min<size_t>(kBruteWarps, fit);
-  *smem = (size_t)*warps * per_warp;
-  return TOS_OK;
 }
 
 __global__ void k_brute_prep(const float* pts, int n, float4* pos, double* wd, double* w) {
@@ -241,95 +265,43 @@ __global__ void k_brute_prep(const float* pts, int n, float4* pos, double* wd, d
   }
 }
 
-// single-block exclusive scan of (wd, w) (n up to a few million: fine for a prep step)
-__global__ void k_brute_scan(const double* wd, const double* w, int n, double2* prefix) {
-  __shared__ double s0[1024], s1[1024];
-  double c0 = 0, c1 = 0;
-  if (threadIdx.x == 0) prefix[0] = make_double2(0, 0);
-  for (int base = 0; base < n; base += 1024) {
-    const int k = base + threadIdx.x;
-    s0[threadIdx.x] = k < n ? wd[k] : 0.0;
-    s1[threadIdx.x] = k < n ? w[k] : 0.0;
-    __syncthreads();
-    for (int d = 1; d < 1024; d <<= 1) {
-      double a0 = 0, a1 = 0;
-      if (threadIdx.x >= (unsigned)d) {
-        a0 = s0[threadIdx.x - d];
-        a1 = s1[threadIdx.x - d];
-      }
-      __syncthreads();
-      s0[threadIdx.x] += a0;
-      s1[threadIdx.x] += a1;
-      __syncthreads();
-    }
-    if (k < n) prefix[k + 1] = make_double2(c0 + s0[threadIdx.x], c1 + s1[threadIdx.x]);
-    c0 += s0[1023];
-    c1 += s1[1023];
-    __syncthreads();
+// 128-bit sums -> the caller's dsum, wsum (FP64) and counts.
+__global__ void k_brute_finish(const unsigned long long* acc, int nb2, double inv0, double inv1, double* dsum,
+                               double* wsum, uint64_t* counts) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb2; b += gridDim.x * blockDim.x) {
+    const unsigned long long* g = acc + (size_t)b * kBWin;
+    const __int128 v0 = (__int128)(long long)g[1] * (__int128)4294967296ll + (__int128)g[0];
+    const __int128 v1 = (__int128)(long long)g[3] * (__int128)4294967296ll + (__int128)g[2];
+    dsum[b] = i128_double(v0) * inv0;
+    wsum[b] = i128_double(v1) * inv1;
+    counts[b] = g[4];
   }
 }
 
-}  // namespace
-}  // namespace tos
+// The kernel's variants, by diagonals per lane.
+struct BruteVariant {
+  int k;
+  void (*fn)(BruteArgs);
+};
+const BruteVariant kVariants[] = {{1, brute_kernel<1>}, {2, brute_kernel<2>}, {4, brute_kernel<4>}};
 
-using namespace tos;
+// Launch shape: per warp a window of kBWin words for each of the nbins + 2
+// bins and a queue of kBQueue runs, so as many warps (up to `warps_max`) as
+// the block's opt-in shared memory holds.  Fails only if not even one warp fits.
+tos_status brute_shape(const tos_engine* e, int nbins, int warps_max, int* warps, size_t* smem) {
+  const size_t per_warp = (size_t)kBWin * (nbins + 2) * 8 + (size_t)kBQueue * sizeof(BRun);
+  const size_t fit = e->smem_optin / per_warp;
+  if (fit < 1)
+    return fail(TOS_ERR_UNSUPPORTED, "nbins too large for one warp's shared-memory window on this device");
+  *warps = (int)std::min<size_t>((size_t)warps_max, fit);
+  *smem = (size_t)*warps * per_warp;
+  return TOS_OK;
+}
 
-extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n_points, double min,
-                                    double max, int nbins, double* dsum, double* wsum,
-                                    uint64_t* counts, double* ms_kernel) {
-  if (!e || !points || !dsum || !wsum || !counts) return fail(TOS_ERR_INVALID_ARG, "null argument");
-  if (n_points < 2 || n_points > (1u << 28)) return fail(TOS_ERR_INVALID_ARG, "need 2 <= n < 2^28 points");
-  if (nbins <= 0 || nbins > 4096) return fail(TOS_ERR_INVALID_ARG, "nbins must be in [1, 4096]");
-  if (!(max > min) || !std::isfinite(min) || !std::isfinite(max))
-    return fail(TOS_ERR_INVALID_ARG, "need finite min < max");
-  std::lock_guard<std::mutex> lock(e->mu);
-  int prev = 0;
-  cudaGetDevice(&prev);
-  cudaSetDevice(e->device);
-  struct Restore {
-    int d;
-    ~Restore() { cudaSetDevice(d); }
-  } restore{prev};
-  const int n = (int)n_points;
-  cudaStream_t st = e->stream;
-  DevBuf<float> d_pts;
-  DevBuf<float4> d_pos;
-  DevBuf<double> d_wd, d_w, d_out;
-  DevBuf<double2> d_prefix;
-  DevBuf<unsigned long long> d_counts, d_misc;
-  TOS_TRY(d_pts.alloc((size_t)n * 5));
-  TOS_TRY(d_pos.alloc(n));
-  TOS_TRY(d_wd.alloc(n));
-  TOS_TRY(d_w.alloc(n));
-  TOS_TRY(d_prefix.alloc((size_t)n + 1));
-  TOS_TRY(d_out.alloc((size_t)(nbins + 2) * 2));
-  TOS_TRY(d_counts.alloc(nbins + 2));
-  TOS_TRY(d_misc.alloc(4));
-  TOS_CUDA_TRY(cudaMemcpyAsync(d_pts.p, points, (size_t)n * 5 * sizeof(float),
-                               cudaMemcpyHostToDevice, st));
-  TOS_CUDA_TRY(cudaMemsetAsync(d_out.p, 0, (size_t)(nbins + 2) * 2 * 8, st));
-  TOS_CUDA_TRY(cudaMemsetAsync(d_counts.p, 0, (size_t)(nbins + 2) * 8, st));
-  TOS_CUDA_TRY(cudaMemsetAsync(d_misc.p, 0, 32, st));
-  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_pts.p, n, d_pos.p, d_wd.p, d_w.p);
-  k_brute_scan<<<1, 1024, 0, st>>>(d_wd.p, d_w.p, n, d_prefix.p);
-  TOS_CUDA_TRY(cudaGetLastError());
-  // bounds of |w*delta| and |w| for the fixed-point scale
-  std::vector<float> hp((size_t)n * 5);
-  std::memcpy(hp.data(), points, hp.size() * sizeof(float));
-  double mwd = 1e-300, mw = 1e-300;
-  for (int k = 0; k < n; ++k) {
-    const double wv = hp[5 * (size_t)k + 4], dv = hp[5 * (size_t)k + 3];
-    if (!std::isfinite(wv) || !std::isfinite(dv) || !std::isfinite(hp[5 * (size_t)k]) ||
-        !std::isfinite(hp[5 * (size_t)k + 1]) || !std::isfinite(hp[5 * (size_t)k + 2]))
-      return fail(TOS_ERR_INVALID_ARG, "points must be finite");
-    mwd = std::max(mwd, std::fabs(wv * dv));
-    mw = std::max(mw, std::fabs(wv));
-  }
-  BruteArgs A{};
-  A.pos = d_pos.p;
-  A.prefix = d_prefix.p;
-  A.wd = d_wd.p;
-  A.w = d_w.p;
+// Fill the kernel arguments shared by both entry points (binning, FP32
+// fast-path constants and the fixed-point scales from the bounds of |w d|
+// and |w|: a run holds at most n - 1 pairs).
+void brute_args(BruteArgs& A, int n, int nbins, double min, double max, double mwd, double mw) {
   A.n = n;
   A.nbins = nbins;
   A.min = min;
@@ -344,40 +316,205 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
   A.k = std::max(0, std::min(13, 21 - bl));
   A.mag = std::ldexp(1.5f, 23 - A.k);
   std::memcpy(&A.bits, &A.mag, 4);
-  const double per[2] = {mwd * kRunCap * mwd, mw * kRunCap * mw};
+  const double per[2] = {mwd * mwd * (double)n, mw * mw * (double)n};
   for (int f = 0; f < 2; ++f) {
-    const int F = (int)std::floor(38.0 - std::log2(per[f]));
-    A.scale[f] = std::ldexp(1.0, F);
-    A.inv_scale[f] = std::ldexp(1.0, -F);
+    int F = (int)std::floor(62.0 - std::log2(std::max(per[f], 1e-300)));
+    F = std::max(-60, std::min(F, 200));
+    A.scale_hi[f] = std::ldexp(1.0, F - 44);
   }
-  A.out = d_out.p;
-  A.counts = d_counts.p;
-  A.next = d_misc.p;
-  A.counters = d_misc.p + 1;
+}
+
+double brute_inv_scale(const BruteArgs& A, int f) { return 1.0 / (A.scale_hi[f] * 17592186044416.0); }
+
+// Launch variant `vi` with up to `warps_max` warps per CTA, persistent (as
+// many CTAs as fit on the SMs), between events ev[4] and ev[5].
+tos_status brute_launch_shape(tos_engine* e, const BruteArgs& A, cudaStream_t st, int vi, int warps_max) {
   int warps = 0;
   size_t smem = 0;
-  TOS_TRY(brute_shape(e, nbins, &warps, &smem));
-  TOS_CUDA_TRY(cudaFuncSetAttribute(brute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+  TOS_TRY(brute_shape(e, A.nbins, warps_max, &warps, &smem));
+  const BruteVariant& v = kVariants[vi];
+  TOS_CUDA_TRY(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  TOS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, warps * 32, smem));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
-  brute_kernel<<<e->num_sms, warps * 32, smem, st>>>(A);
+  v.fn<<<e->num_sms * std::max(1, per_sm), warps * 32, smem, st>>>(A);
   TOS_CUDA_TRY(cudaGetLastError());
   TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
-  std::vector<double> out((size_t)(nbins + 2) * 2);
-  std::vector<unsigned long long> cnt(nbins + 2);
-  TOS_CUDA_TRY(cudaMemcpyAsync(out.data(), d_out.p, out.size() * 8, cudaMemcpyDeviceToHost, st));
-  TOS_CUDA_TRY(cudaMemcpyAsync(cnt.data(), d_counts.p, cnt.size() * 8, cudaMemcpyDeviceToHost, st));
-  TOS_CUDA_TRY(cudaStreamSynchronize(st));
-  for (int b = 0; b < nbins + 2; ++b) {
-    dsum[b] = out[2 * b];
-    wsum[b] = out[2 * b + 1];
-    counts[b] = cnt[b];
+  return TOS_OK;
+}
+
+// The default shape, or the one tos_brute_tune picked for this bin count.
+constexpr int kBruteDefaultVariant = 0, kBruteDefaultWarps = 8;
+
+tos_status brute_launch(tos_engine* e, const BruteArgs& A, cudaStream_t st) {
+  int vi = kBruteDefaultVariant, warps_max = kBruteDefaultWarps;
+  {
+    std::lock_guard<std::mutex> lk(e->tune_mu);
+    auto it = e->brute_tuned.find(A.nbins);
+    if (it != e->brute_tuned.end()) {
+      vi = it->second.first;
+      warps_max = it->second.second;
+    }
   }
+  return brute_launch_shape(e, A, st, vi, warps_max);
+}
+
+}  // namespace
+}  // namespace tos
+
+using namespace tos;
+
+extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n_points, double min,
+                                    double max, int nbins, double* dsum, double* wsum,
+                                    uint64_t* counts, double* ms_kernel) {
+  if (!e || !points || !dsum || !wsum || !counts) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (n_points < 2 || n_points > (1u << 24)) return fail(TOS_ERR_INVALID_ARG, "need 2 <= n <= 2^24 points");
+  if (nbins <= 0 || nbins > 4096) return fail(TOS_ERR_INVALID_ARG, "nbins must be in [1, 4096]");
+  if (!(max > min) || !std::isfinite(min) || !std::isfinite(max))
+    return fail(TOS_ERR_INVALID_ARG, "need finite min < max");
+  // bounds of |w*delta| and |w| for the fixed-point scale
+  const int n = (int)n_points;
+  double mwd = 1e-300, mw = 1e-300;
+  for (int k = 0; k < n; ++k) {
+    const float* p = points + 5 * (size_t)k;
+    if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2]) || !std::isfinite(p[3]) ||
+        !std::isfinite(p[4]))
+      return fail(TOS_ERR_INVALID_ARG, "points must be finite");
+    mwd = std::max(mwd, std::fabs((double)p[4] * (double)p[3]));
+    mw = std::max(mw, std::fabs((double)p[4]));
+  }
+  std::lock_guard<std::mutex> lock(e->mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(e->device);
+  struct Restore {
+    int d;
+    ~Restore() { cudaSetDevice(d); }
+  } restore{prev};
+  const int nb2 = nbins + 2;
+  cudaStream_t st = e->stream;
+  DevBuf<float> d_pts;
+  DevBuf<float4> d_pos;
+  DevBuf<double> d_wd, d_w, d_out;
+  DevBuf<unsigned long long> d_acc, d_misc;
+  DevBuf<uint64_t> d_cnt;
+  TOS_TRY(d_pts.alloc((size_t)n * 5));
+  TOS_TRY(d_pos.alloc(n));
+  TOS_TRY(d_wd.alloc(n));
+  TOS_TRY(d_w.alloc(n));
+  TOS_TRY(d_acc.alloc((size_t)nb2 * kBWin));
+  TOS_TRY(d_out.alloc((size_t)nb2 * 2));
+  TOS_TRY(d_cnt.alloc(nb2));
+  TOS_TRY(d_misc.alloc(4));
+  TOS_CUDA_TRY(cudaMemcpyAsync(d_pts.p, points, (size_t)n * 5 * sizeof(float),
+                               cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemsetAsync(d_acc.p, 0, (size_t)nb2 * kBWin * 8, st));
+  TOS_CUDA_TRY(cudaMemsetAsync(d_misc.p, 0, 32, st));
+  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_pts.p, n, d_pos.p, d_wd.p, d_w.p);
+  TOS_CUDA_TRY(cudaGetLastError());
+  BruteArgs A{};
+  A.pos = d_pos.p;
+  A.wd = d_wd.p;
+  A.w = d_w.p;
+  brute_args(A, n, nbins, min, max, mwd, mw);
+  A.acc = d_acc.p;
+  A.next = d_misc.p;
+  A.counters = d_misc.p + 1;
+  TOS_TRY(brute_launch(e, A, st));
+  k_brute_finish<<<(nb2 + 127) / 128, 128, 0, st>>>(d_acc.p, nb2, brute_inv_scale(A, 0), brute_inv_scale(A, 1),
+                                                   d_out.p, d_out.p + nb2, d_cnt.p);
+  TOS_CUDA_TRY(cudaGetLastError());
+  TOS_CUDA_TRY(cudaMemcpyAsync(dsum, d_out.p, (size_t)nb2 * 8, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(wsum, d_out.p + nb2, (size_t)nb2 * 8, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(counts, d_cnt.p, (size_t)nb2 * 8, cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
   if (ms_kernel) {
     float ms = 0;
     cudaEventElapsedTime(&ms, e->ev[4], e->ev[5]);
     *ms_kernel = ms;
   }
+  return TOS_OK;
+}
+
+// Autotuner of the brute-force kernel's launch shape: every variant (1, 2 or
+// 4 diagonals per lane) with 4, 8 and 16 warps per CTA, timed on the first
+// min(n, 131072) points, best of two timed launches after a warm-up.
+extern "C" tos_status tos_brute_tune(tos_engine* e, const float* points, size_t n_points, double min,
+                                     double max, int nbins, int* diagonals_per_lane, int* warps_per_cta) {
+  if (!e || !points) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (n_points < 2 || n_points > (1u << 24)) return fail(TOS_ERR_INVALID_ARG, "need 2 <= n <= 2^24 points");
+  if (nbins <= 0 || nbins > 4096) return fail(TOS_ERR_INVALID_ARG, "nbins must be in [1, 4096]");
+  if (!(max > min) || !std::isfinite(min) || !std::isfinite(max))
+    return fail(TOS_ERR_INVALID_ARG, "need finite min < max");
+  const int n = (int)std::min<size_t>(n_points, 131072);
+  double mwd = 1e-300, mw = 1e-300;
+  for (int k = 0; k < n; ++k) {
+    const float* p = points + 5 * (size_t)k;
+    if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2]) || !std::isfinite(p[3]) ||
+        !std::isfinite(p[4]))
+      return fail(TOS_ERR_INVALID_ARG, "points must be finite");
+    mwd = std::max(mwd, std::fabs((double)p[4] * (double)p[3]));
+    mw = std::max(mw, std::fabs((double)p[4]));
+  }
+  std::lock_guard<std::mutex> lock(e->mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(e->device);
+  struct Restore {
+    int d;
+    ~Restore() { cudaSetDevice(d); }
+  } restore{prev};
+  const int nb2 = nbins + 2;
+  cudaStream_t st = e->stream;
+  DevBuf<float> d_pts;
+  DevBuf<float4> d_pos;
+  DevBuf<double> d_wd, d_w;
+  DevBuf<unsigned long long> d_acc, d_misc;
+  TOS_TRY(d_pts.alloc((size_t)n * 5));
+  TOS_TRY(d_pos.alloc(n));
+  TOS_TRY(d_wd.alloc(n));
+  TOS_TRY(d_w.alloc(n));
+  TOS_TRY(d_acc.alloc((size_t)nb2 * kBWin));
+  TOS_TRY(d_misc.alloc(4));
+  TOS_CUDA_TRY(cudaMemcpyAsync(d_pts.p, points, (size_t)n * 5 * sizeof(float), cudaMemcpyHostToDevice, st));
+  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_pts.p, n, d_pos.p, d_wd.p, d_w.p);
+  TOS_CUDA_TRY(cudaGetLastError());
+  BruteArgs A{};
+  A.pos = d_pos.p;
+  A.wd = d_wd.p;
+  A.w = d_w.p;
+  brute_args(A, n, nbins, min, max, mwd, mw);
+  A.acc = d_acc.p;
+  A.next = d_misc.p;
+  A.counters = d_misc.p + 1;
+  const int warp_opts[3] = {4, 8, 16};
+  float best = 0.f;
+  int best_v = kBruteDefaultVariant, best_w = kBruteDefaultWarps;
+  for (int vi = 0; vi < (int)(sizeof(kVariants) / sizeof(kVariants[0])); ++vi) {
+    for (int wo : warp_opts) {
+      float t_min = 0.f;
+      for (int rep = 0; rep < 3; ++rep) {
+        TOS_CUDA_TRY(cudaMemsetAsync(d_acc.p, 0, (size_t)nb2 * kBWin * 8, st));
+        TOS_CUDA_TRY(cudaMemsetAsync(d_misc.p, 0, 32, st));
+        TOS_TRY(brute_launch_shape(e, A, st, vi, wo));
+        TOS_CUDA_TRY(cudaEventSynchronize(e->ev[5]));
+        float ms = 0.f;
+        TOS_CUDA_TRY(cudaEventElapsedTime(&ms, e->ev[4], e->ev[5]));
+        if (rep > 0 && (rep == 1 || ms < t_min)) t_min = ms;
+      }
+      if (best == 0.f || t_min < best) {
+        best = t_min;
+        best_v = vi;
+        best_w = wo;
+      }
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(e->tune_mu);
+    e->brute_tuned[nbins] = std::make_pair(best_v, best_w);
+  }
+  if (diagonals_per_lane) *diagonals_per_lane = kVariants[best_v].k;
+  if (warps_per_cta) *warps_per_cta = best_w;
   return TOS_OK;
 }
 
@@ -404,11 +541,9 @@ constexpr size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 constexpr size_t kNaPos = 0;                                                  // float4[n]
 constexpr size_t kNaWd = kNaPos + round256(16 * kNoAllocMaxPoints);           // double[n]
 constexpr size_t kNaW = kNaWd + round256(8 * kNoAllocMaxPoints);              // double[n]
-constexpr size_t kNaPrefix = kNaW + round256(8 * kNoAllocMaxPoints);          // double2[n + 1]
-constexpr size_t kNaOut = kNaPrefix + round256(16 * (kNoAllocMaxPoints + 1));  // double[2 (nbins + 2)]
-constexpr size_t kNaCounts = kNaOut + round256(16 * (kNoAllocMaxBins + 2));   // u64[nbins + 2]
-constexpr size_t kNaMisc = kNaCounts + round256(8 * (kNoAllocMaxBins + 2));   // u64[8]
-constexpr size_t kNoAllocBytes = kNaMisc + 256;                               // ~12.7 MB
+constexpr size_t kNaAcc = kNaW + round256(8 * kNoAllocMaxPoints);             // u64[nbins + 2][kBWin]
+constexpr size_t kNaMisc = kNaAcc + round256(8 * kBWin * (kNoAllocMaxBins + 2));  // u64[8]
+constexpr size_t kNoAllocBytes = kNaMisc + 256;                               // ~8.5 MB
 
 // The scratch.  Host code must not pass this name to a kernel: on the host
 // it stands for a host-side shadow, not for the device memory; the device
@@ -437,16 +572,6 @@ __global__ void k_brute_bounds(const float* pts, int n, unsigned long long* maxb
     atomicMax(&maxbits[0], (unsigned long long)__double_as_longlong(mwd));
     atomicMax(&maxbits[1], (unsigned long long)__double_as_longlong(mw));
     if (nonfinite) atomicOr(bad, 1ull);
-  }
-}
-
-// interleaved (dsum, wsum) sums and counts -> the caller's three arrays
-__global__ void k_brute_unpack(const double* out, const unsigned long long* cnt, int nb2, double* dsum,
-                               double* wsum, uint64_t* counts) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb2; b += gridDim.x * blockDim.x) {
-    dsum[b] = out[2 * b];
-    wsum[b] = out[2 * b + 1];
-    counts[b] = cnt[b];
   }
 }
 
@@ -501,18 +626,14 @@ extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points
   float4* pos = (float4*)(S + kNaPos);
   double* wd = (double*)(S + kNaWd);
   double* w = (double*)(S + kNaW);
-  double2* prefix = (double2*)(S + kNaPrefix);
-  double* out = (double*)(S + kNaOut);
-  unsigned long long* cnt = (unsigned long long*)(S + kNaCounts);
-  unsigned long long* misc = (unsigned long long*)(S + kNaMisc);  // [0] chunk counter [1] rechecks
+  unsigned long long* acc = (unsigned long long*)(S + kNaAcc);
+  unsigned long long* misc = (unsigned long long*)(S + kNaMisc);  // [0] group counter [1] rechecks
                                                                    // [2,3] bounds [4] non-finite
   // the scratch keeps the previous call's contents: clear what accumulates
-  TOS_CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)nb2 * 2 * sizeof(double), st));
-  TOS_CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)nb2 * sizeof(unsigned long long), st));
+  TOS_CUDA_TRY(cudaMemsetAsync(acc, 0, (size_t)nb2 * kBWin * sizeof(unsigned long long), st));
   TOS_CUDA_TRY(cudaMemsetAsync(misc, 0, 8 * sizeof(unsigned long long), st));
   k_brute_bounds<<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(d_points, n, misc + 2, misc + 4);
   k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_points, n, pos, wd, w);
-  k_brute_scan<<<1, 1024, 0, st>>>(wd, w, n, prefix);
   TOS_CUDA_TRY(cudaGetLastError());
   unsigned long long hb[3] = {0, 0, 0};
   TOS_CUDA_TRY(cudaMemcpyAsync(hb, misc + 2, sizeof(hb), cudaMemcpyDeviceToHost, st));
@@ -523,46 +644,18 @@ extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points
   std::memcpy(&mw, &hb[1], 8);
   mwd = std::max(mwd, 1e-300);
   mw = std::max(mw, 1e-300);
-  // the same kernel arguments as tos_brute_run, pointing into the scratch
+  // the same kernel and arguments as tos_brute_run, pointing into the scratch
   BruteArgs A{};
   A.pos = pos;
-  A.prefix = prefix;
   A.wd = wd;
   A.w = w;
-  A.n = n;
-  A.nbins = nbins;
-  A.min = min;
-  A.max = max;
-  A.spacing = (max - min) / nbins;
-  A.invf = (float)(1.0 / A.spacing);
-  A.offf = (float)(-min / A.spacing);
-  A.nbf = (float)nbins;
-  A.nbp1f = (float)nbins + 1.0f;
-  int bl = 0;
-  for (uint32_t v = (uint32_t)nbins + 2; v; v >>= 1) ++bl;
-  A.k = std::max(0, std::min(13, 21 - bl));
-  A.mag = std::ldexp(1.5f, 23 - A.k);
-  std::memcpy(&A.bits, &A.mag, 4);
-  const double per[2] = {mwd * kRunCap * mwd, mw * kRunCap * mw};
-  for (int f = 0; f < 2; ++f) {
-    const int F = (int)std::floor(38.0 - std::log2(per[f]));
-    A.scale[f] = std::ldexp(1.0, F);
-    A.inv_scale[f] = std::ldexp(1.0, -F);
-  }
-  A.out = out;
-  A.counts = cnt;
+  brute_args(A, n, nbins, min, max, mwd, mw);
+  A.acc = acc;
   A.next = misc;
   A.counters = misc + 1;
-  int warps = 0;
-  size_t smem = 0;
-  TOS_TRY(brute_shape(e, nbins, &warps, &smem));
-  TOS_CUDA_TRY(cudaFuncSetAttribute(brute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-  TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
-  brute_kernel<<<e->num_sms, warps * 32, smem, st>>>(A);
-  TOS_CUDA_TRY(cudaGetLastError());
-  TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
-  k_brute_unpack<<<(nb2 + 255) / 256, 256, 0, st>>>(out, cnt, nb2, d_dsum, d_wsum, d_counts);
+  TOS_TRY(brute_launch(e, A, st));
+  k_brute_finish<<<(nb2 + 127) / 128, 128, 0, st>>>(acc, nb2, brute_inv_scale(A, 0), brute_inv_scale(A, 1),
+                                                   d_dsum, d_wsum, d_counts);
   TOS_CUDA_TRY(cudaGetLastError());
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
   if (ms_kernel) {

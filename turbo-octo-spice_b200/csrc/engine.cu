@@ -500,16 +500,23 @@ __global__ void k_grid_first(const float* xpad, const uint64_t* off, const uint3
   }
 }
 
-// Boundary table Q[side][g][k] = first grid index g2 whose value x2 = U[g2]
-// passes the boundary predicate of threshold T[k] against x1 = U[g]:
-//   side 0: x2 >= x1 and fl(x2 - x1) >= T[k];  side 1: x2 >= x1 or fl(x1 - x2) < T[k].
+// Boundary table B[g][t], t = 0 .. 2 nk - 1 (nk = n0 + 1 thresholds): the
+// first grid index g2 whose value x2 = U[g2] passes the boundary predicate of
+// threshold T[k] against x1 = U[g],
+//   side 1, t <= n0 (k = n0 - t):      x2 >= x1 or  fl(x1 - x2) <  T[k];
+//   side 0, t = n0 + 1 + k:            x2 >= x1 and fl(x2 - x1) >= T[k].
+// Along t the entries are non-decreasing, so the row's columns split into the
+// consecutive runs [B[t], B[t+1]): first-axis bin n0 - 1 - t below x1
+// (t < n0), the |x1 - x2| < T[0] gap (t = n0), bin t - n0 - 1 above x1.
 __global__ void k_grid_table(const float* U, int ng, const float* thr, int nk, uint16_t* Q) {
-  const size_t total = (size_t)2 * ng * nk;
+  const int nb = 2 * nk;
+  const size_t total = (size_t)ng * nb;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
        e += (size_t)gridDim.x * blockDim.x) {
-    const int k = (int)(e % nk);
-    const int g = (int)((e / nk) % ng);
-    const int side = (int)(e / ((size_t)nk * ng));
+    const int tb = (int)(e % nb);
+    const int g = (int)(e / nb);
+    const int side = tb < nk ? 1 : 0;
+    const int k = side ? nk - 1 - tb : tb - nk;
     const float x1 = U[g], t = thr[k];
     int lo = 0, hi = ng;
     while (lo < hi) {
@@ -917,6 +924,23 @@ size_t Workspace::bytes() const {
          d_counters.bytes() + d_thr.bytes() + d_gq.bytes() + d_cub_tmp.bytes();
 }
 
+// Fixed-point scales for kernels whose FP64 register sums can hold a whole
+// item's pairs of a bin (at most max_np^2 pairs): every field takes the wide
+// 62-bit conversion (the run, grid and diagonal sweeps).
+static void set_wide_scales(PairArgs& A, const tos_catalog* cat) {
+  const double m = std::max<double>(1.0, cat->max_np);
+  const double wdm = std::max(cat->max_abs_wd, 1e-300), wm = std::max(cat->max_w, 1e-300),
+               lm = std::max(cat->max_l, 1e-300);
+  const double bound[7] = {wdm * m * wdm, wdm * m, m * wdm, wm * m * wm, wm * m, m * wm, lm * m};
+  for (int k = 0; k < 7; ++k) {
+    int f = (int)std::floor(62.0 - std::log2(bound[k] * m));
+    f = std::max(-60, std::min(f, 200));
+    A.scale[k] = std::ldexp(1.0, f);
+    A.scale_hi[k] = std::ldexp(1.0, f - 44);
+  }
+  A.wide_all = 1;
+}
+
 tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos_grid* grid,
                        double scale, uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
                        tos_xibin* out_cells, tos_xi_stats* stats) {
@@ -1235,19 +1259,7 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
       TOS_CUDA_TRY(cudaMemcpyAsync(ws->d_thr.p, thr.data(), (n0 + 1) * sizeof(float),
                                    cudaMemcpyHostToDevice, st));
       A.thr = ws->d_thr.p;
-      // one FP64 register sum can hold a whole item's pairs of a bin
-      // (at most max_np^2): every field takes the wide 62-bit conversion
-      const double m = std::max<double>(1.0, cat->max_np);
-      const double wdm = std::max(cat->max_abs_wd, 1e-300), wm = std::max(cat->max_w, 1e-300),
-                   lm = std::max(cat->max_l, 1e-300);
-      const double bound[7] = {wdm * m * wdm, wdm * m, m * wdm, wm * m * wm, wm * m, m * wm, lm * m};
-      for (int k = 0; k < 7; ++k) {
-        int f = (int)std::floor(62.0 - std::log2(bound[k] * m));
-        f = std::max(-60, std::min(f, 200));
-        A.scale[k] = std::ldexp(1.0, f);
-        A.scale_hi[k] = std::ldexp(1.0, f - 44);
-      }
-      A.wide_all = 1;
+      set_wide_scales(A, cat);
       A.run_split = 1;
     }
   }
@@ -1270,8 +1282,30 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
       use_grid = true;
     }
   }
+  // --- diagonal sweep (Polar, sorted sightlines): every item whose z index is
+  // constant.  Its lanes add one run of pairs at a time, so the adds to one
+  // (row, bin) are at most the row's pixel pairs, which must stay below the
+  // 2^32 adds the carry-free sums take.
+  bool use_diag = false;
+  if (G.type == TOS_POLAR && cat->sorted && !A.force_exact && n_items > 0) {
+    const uint64_t max_row_pairs =
+        plan ? plan->max_row_items(std::vector<uint64_t>(cell_pairs.begin(), cell_pairs.end())) : max_cell_pairs;
+    if (max_row_pairs < (1ull << 32)) {
+      set_wide_scales(A, cat);
+      A.diag_split = 1;
+      use_diag = true;
+    }
+  }
   if (n_items > 0) {
     TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    if (use_diag) {
+      PairArgs R = A;
+      R.next_item = ctr + 11;
+      const cudaError_t de = launch_diag_kernel(R, minpos, e->num_sms, st);
+      if (de != cudaSuccess)
+        return fail(TOS_ERR_CUDA, std::string("diagonal kernel: ") + cudaGetErrorString(de));
+    }
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[7], st));
     if (use_grid) {
       PairArgs R = A;
       R.next_item = ctr + 10;
@@ -1294,6 +1328,7 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
     TOS_CUDA_TRY(cudaEventRecord(e->ev[3], st));
   } else {
     TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
+    TOS_CUDA_TRY(cudaEventRecord(e->ev[7], st));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[6], st));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[3], st));
@@ -1326,7 +1361,7 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
   if (n_rows)
     TOS_CUDA_TRY(cudaMemcpyAsync(out_cells, ws->d_out.p + nb, n_rows * nb * sizeof(tos_xibin),
                                  cudaMemcpyDeviceToHost, st));
-  unsigned long long hc[10];
+  unsigned long long hc[13];
   TOS_CUDA_TRY(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
   TOS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1358,12 +1393,15 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
     stats->ms_pairs = ms;
     cudaEventElapsedTime(&ms, e->ev[0], e->ev[4]);
     stats->ms_device = ms;
-    cudaEventElapsedTime(&ms, e->ev[2], e->ev[5]);
+    cudaEventElapsedTime(&ms, e->ev[7], e->ev[5]);
     stats->ms_runs = ms;
-    cudaEventElapsedTime(&ms, e->ev[2], e->ev[6]);
+    cudaEventElapsedTime(&ms, e->ev[7], e->ev[6]);
     stats->ms_grid = ms;
     stats->num_run_items = hc[8] + hc[9];
     stats->num_grid_items = hc[9];
+    cudaEventElapsedTime(&ms, e->ev[2], e->ev[7]);
+    stats->ms_diag = ms;
+    stats->num_diag_items = hc[12];
     stats->ms_total =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   }

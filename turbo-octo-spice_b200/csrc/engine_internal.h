@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -97,8 +98,12 @@ struct tos_engine {
   int num_sms = 0;
   size_t smem_optin = 0;  // opt-in shared memory per block (bytes)
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[7] = {};
+  cudaEvent_t ev[8] = {};
   std::mutex mu;
+  // launch shapes picked by the autotuner (tos_brute_tune), by bin count:
+  // (kernel variant, warps per CTA)
+  std::mutex tune_mu;
+  std::map<int, std::pair<int, int>> brute_tuned;
 };
 
 struct tos_catalog {

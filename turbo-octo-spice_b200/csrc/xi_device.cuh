@@ -121,5 +121,14 @@ __device__ __forceinline__ uint32_t zbin_of_sum(float lsum, const RefGrid& g) {
   return ref_u32(dmul(dsub(dmul(0.5, (double)lsum), g.min2), g.invn2));
 }
 
+// Items of the diagonal-sweep kernel when A.diag_split is set (Polar): the z
+// index is constant over the item (from the z codes zlo, zhi of the smallest
+// and largest loglam sums and their indices).  Both the diagonal-sweep and
+// the pixel-pair kernel evaluate this same predicate.
+__device__ __forceinline__ bool diag_item(const PairArgs& A, double zlo, double zhi, uint32_t zb_lo,
+                                          uint32_t zb_hi) {
+  return A.diag_split && zlo > -1.0 && zhi < 2147483648.0 && zb_lo == zb_hi;
+}
+
 }  // namespace
 }  // namespace tos

@@ -6,12 +6,14 @@
 // With U the sorted distinct first-axis values of the catalogue and a
 // sightline contiguous on U (its pixel p has value U[f + p]), the run
 // boundaries of xi_sweep.cuh for a row x1 = U[g] along any column sightline j
-// are
-//   q_k = clamp(Q[side][g][k] - f_j, 0, n_j),
-// where Q[side][g][k] is the first grid index g2 whose value passes the
-// boundary predicate of threshold T[k] against U[g].  Q is built once per
-// call (k_grid_table, engine.cu), so a lane reads both ends of its run with
-// two adjacent table loads instead of walking pointers.
+// are the entries of one table row, in column order:
+//   B[g][t] - f_j clamped to [0, n_j],  t = 0 .. 2 n0 + 1,
+// where B[g][t] is the first grid index g2 whose value passes the boundary
+// predicate of a threshold T[k] against U[g] (side 1 for t <= n0, side 0
+// after it; k_grid_table, engine.cu).  The row's columns are then the
+// consecutive runs [B[t], B[t+1]), t = 0 .. 2 n0, each of one first-axis bin
+// (run n0 is the |x1 - x2| < T[0] gap), so neighbouring lanes share a
+// boundary: a lane reads one table entry per row and evaluates one column.
 #include "xi_sweep.cuh"
 
 namespace tos {
@@ -19,21 +21,96 @@ namespace {
 
 constexpr int kGridWarps = 4;  // warps per CTA of the grid-sweep kernel
 
-// Rows [r_lo, r_hi) of an item for the (side, bin) tasks t0 .. t0 + m - 1
-// (m = min(32, tasks left)).  A group of m < 32 tasks splits the rows into
-// P = 32 / m phases: lane = task + m * phase takes rows r_lo + phase + P i,
-// so the last, partial group of a grid costs 1/P of a full pass.
+// Runs of an item per pass: a pass holds m + 1 <= 32 consecutive boundaries
+// of a row, so it owns m runs.
+constexpr int kPassRuns = 31;
+constexpr int kGridThreads = kGridWarps * 32;
+
+// A grid-sweep lane's FP64 sums (7 XiBin sums and the pair count) of its run
+// for two r_perp codes: the current code C in registers and C - 1 in shared
+// memory.  Along the rows of an item a run's code grows slowly; the rows
+// where the run straddles a code edge add to both.  A code leaves for the
+// per-cell sums once, when the codes move past it; a code below C - 1 (rare)
+// goes straight out.  Same adds per (item, bin) as RunAcc.
+struct GridAcc {
+  int C;             // code of the register sums (-1: nothing added yet)
+  bool prev_used;    // the shared sums of code C - 1 hold something
+  double s[8];
+  double* prev;      // this lane's shared sums of code C - 1, field f at prev[f * kGridThreads]
+
+  template <int COORD>
+  __device__ __forceinline__ void flush_prev(const PairArgs& A, Dest d, int k) {
+    if (!prev_used) return;
+    double v[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) v[f] = prev[f * kGridThreads];
+    acc_flush8<COORD>(A, d, k, C - 1, v);
+    prev_used = false;
+  }
+
+  template <int COORD>
+  __device__ __forceinline__ void add(const PairArgs& A, Dest d, int k, int cc, const double (&v)[8]) {
+    if (C < 0) C = cc;
+    if (cc == C) {
+#pragma unroll
+      for (int f = 0; f < 8; ++f) s[f] += v[f];
+    } else if (cc == C - 1) {
+#pragma unroll
+      for (int f = 0; f < 8; ++f) prev[f * kGridThreads] = (prev_used ? prev[f * kGridThreads] : 0.0) + v[f];
+      prev_used = true;
+    } else if (cc == C + 1) {
+      flush_prev<COORD>(A, d, k);
+#pragma unroll
+      for (int f = 0; f < 8; ++f) {
+        prev[f * kGridThreads] = s[f];
+        s[f] = v[f];
+      }
+      prev_used = true;
+      C = cc;
+    } else if (cc > C + 1) {
+      flush_prev<COORD>(A, d, k);
+      acc_flush8<COORD>(A, d, k, C, s);
+#pragma unroll
+      for (int f = 0; f < 8; ++f) s[f] = v[f];
+      C = cc;
+    } else {
+      acc_flush8<COORD>(A, d, k, cc, v);  // below both codes: straight out
+    }
+  }
+
+  template <int COORD>
+  __device__ __forceinline__ void finish(const PairArgs& A, Dest d, int k) {
+    flush_prev<COORD>(A, d, k);
+    if (C >= 0) acc_flush8<COORD>(A, d, k, C, s);
+  }
+};
+
+// One pass over the rows of an item: runs t0 .. t0 + m - 1 of every row,
+// run t = [B[t], B[t+1]) of the row's boundary table (k_grid_table, engine.cu)
+// with the columns clamped to sightline j.  Boundary b (0 <= b <= m) of the
+// pass sits on lane b + (m + 1) q of phase q = 0 .. P - 1, P = 32 / (m + 1);
+// phase q takes rows g_lo + q, g_lo + q + P, ...  A lane evaluates its own
+// boundary only: the column, its r_perp code and sightline j's prefix sums
+// there.  The lane of boundary b owns run t0 + b and reads the run's far end
+// from lane b + 1: when the two codes agree, every column of the run has that
+// code (the code is non-decreasing along a row), so the run is added from the
+// two prefix sums without evaluating anything else; otherwise the far end is
+// evaluated and the run split by bisection.  Each lane sums its run into FP64
+// registers across the rows (its first-axis bin is fixed; its r_perp code
+// moves slowly from row to row) and adds them to the per-cell sums when its
+// codes move on.
 template <int COORD, bool MINPOS>
-__device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, int fi, int fj,
-                                        int t0, int lane, unsigned long long* stats) {
+__device__ __noinline__ void grid_pass(const PairArgs& A, const SweepItem& it, int fi, int fj, int t0,
+                                       int m, int lane, double* prev, unsigned long long* stats) {
   const int n0 = (int)A.g.n0;
-  const int m = min(32, 2 * n0 - t0);
-  const int P = 32 / m;
-  const bool act = lane < m * P;
-  const int task = t0 + (act ? lane % m : 0);
-  const int phase = act ? lane / m : 0;
-  const int side = task / n0;
-  const int k = task % n0;
+  const int nbd = 2 * n0 + 2;  // boundaries per table row
+  const int P = 32 / (m + 1);
+  const bool act = lane < (m + 1) * P;
+  const int bi = act ? lane % (m + 1) : m;
+  const int phase = act ? lane / (m + 1) : 0;
+  const int t = t0 + bi;
+  const bool owner = act && bi < m && t != n0;  // run n0 is the |x1 - x2| < T[0] gap
+  const int k = (t < n0) ? n0 - 1 - t : t - n0 - 1;
   // the item in registers: the loop's flushes would force reloads from memory
   const int nj = it.nj, r_lo = it.r_lo, r_hi = it.r_hi;
   const Dest d = it.d;
@@ -42,71 +119,81 @@ __device__ __noinline__ void grid_group(const PairArgs& A, const SweepItem& it, 
   const float *rowd = it.rowd, *rowl = it.rowl, *roww = it.roww, *colx = it.colx;
   const double* rowwd = it.rowwd;
   const double4* pre = it.pre;
-  const size_t qstride = (size_t)(n0 + 1);
-  const uint16_t* qrow = A.gq + ((size_t)side * A.ng + fi) * qstride + k;
-  RunAcc acc;
-  acc.B = -1;
+  const uint16_t* tab = A.gq + (size_t)fi * nbd;  // row r: tab[r * nbd + t]
+  // Rows where a run of the pass is non-empty: B[t0 + m] > fj and
+  // B[t0] < fj + nj.  Table entries are non-decreasing along the rows, so
+  // these rows form one interval (found the same way by every lane).
+  int g_lo = r_lo, g_hi = r_hi;
+  {
+    int b = r_hi;
+    while (g_lo < b) {
+      const int mid = (g_lo + b) >> 1;
+      if ((int)tab[(size_t)mid * nbd + t0 + m] > fj) b = mid; else g_lo = mid + 1;
+    }
+    int a = g_lo;
+    while (a < g_hi) {
+      const int mid = (a + g_hi) >> 1;
+      if ((int)tab[(size_t)mid * nbd + t0] >= fj + nj) g_hi = mid; else a = mid + 1;
+    }
+  }
+  if (g_hi <= g_lo) return;  // warp-uniform: every run of the pass is empty
+  GridAcc acc;
+  acc.C = -1;
+  acc.prev_used = false;
+  acc.prev = prev;
 #pragma unroll
-  for (int f = 0; f < 8; ++f) acc.s0[f] = acc.s1[f] = 0.0;
+  for (int f = 0; f < 8; ++f) acc.s[f] = 0.0;
   unsigned rech = 0;
   unsigned long long n_eval = 0;
-  // Rows where some task of the group has a non-empty run.  Table entries are
-  // non-decreasing along the rows, so the run of (side, k) is non-empty on
-  // one row interval: side 0 [Q_k, Q_k+1) needs Q_k+1 > fj and Q_k < fj + nj,
-  // side 1 [Q_k+1, Q_k) needs Q_k > fj and Q_k+1 < fj + nj.
-  int g_lo = r_hi, g_hi = r_lo;
-  if (act) {
-    const int lo_col = side ? 0 : 1, hi_col = side ? 1 : 0;
-    int a = r_lo, b = r_hi;  // first row with Q[lo_col] > fj
-    while (a < b) {
-      const int mid = (a + b) >> 1;
-      if ((int)qrow[(size_t)mid * qstride + lo_col] > fj) b = mid; else a = mid + 1;
-    }
-    int c2 = a, d2 = r_hi;  // first row with Q[hi_col] >= fj + nj
-    while (c2 < d2) {
-      const int mid = (c2 + d2) >> 1;
-      if ((int)qrow[(size_t)mid * qstride + hi_col] >= fj + nj) d2 = mid; else c2 = mid + 1;
-    }
-    g_lo = a;
-    g_hi = c2;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    g_lo = min(g_lo, __shfl_xor_sync(kFull, g_lo, o));
-    g_hi = max(g_hi, __shfl_xor_sync(kFull, g_hi, o));
-  }
-  if (g_hi <= g_lo) return;  // warp-uniform: every run of the group is empty
-  // boundaries loaded one row ahead
-  const int r0 = min(g_lo + phase, g_hi - 1);
-  ushort2 nQ = make_ushort2(qrow[(size_t)r0 * qstride], qrow[(size_t)r0 * qstride + 1]);
-  RowV nR = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, r0);
+  const int n1 = (int)A.g.n1;
+  const int iters = (g_hi - g_lo + P - 1) / P;  // the same for every phase (shuffles below)
+  const uint16_t* tcol = tab + t;
+  int r = g_lo + phase;
+  // the next row's boundary and row values, loaded a row ahead
+  int r0 = min(r, g_hi - 1);
+  int nb = min(max((int)tcol[(size_t)r0 * nbd] - fj, 0), nj);
+  RowRaw nR = row_raw(rowd, rowwd, roww, rowl, r0);
 #pragma unroll 1
-  for (int r = g_lo + phase; r < g_hi; r += P) {
-    const ushort2 Qv = nQ;
-    const RowV R = nR;
+  for (int q = 0; q < iters; ++q, r += P) {
+    const bool valid = act && r < g_hi;
+    const int b = nb;
+    const RowV R = row_derive<COORD>(nR, ap, inv1sqf);
     const int rn = min(r + P, g_hi - 1);
-    nQ = make_ushort2(qrow[(size_t)rn * qstride], qrow[(size_t)rn * qstride + 1]);
-    nR = row_values<COORD>(rowd, rowwd, roww, rowl, ap, inv1sqf, rn);
-    const int qa = min(max((int)Qv.x - fj, 0), nj), qb = min(max((int)Qv.y - fj, 0), nj);
-    const int s = side ? qb : qa, e = side ? qa : qb;
-    if (act && e > s) {
-      n_eval += (unsigned long long)(e - s);
-      do_run<COORD, MINPOS>(A, d, colx, pre, c, R, k, s, e, acc, rech);
+    nb = min(max((int)tcol[(size_t)rn * nbd] - fj, 0), nj);
+    nR = row_raw(rowd, rowwd, roww, rowl, rn);
+    // this lane's boundary: r_perp code of column b (of the last column when
+    // b = nj: then it is the code of the last column of the run ending here)
+    int code = 0;
+    if (COORD == kCart && valid) code = perp_code<MINPOS>(A, R, colx[min(b, nj - 1)], c, rech);
+    const double2 pwd = *reinterpret_cast<const double2*>(&pre[b]);
+    const double pl = pre[b].z;
+    const int be = __shfl_down_sync(kFull, b, 1);
+    const int ce = __shfl_down_sync(kFull, code, 1);
+    const double ewd = __shfl_down_sync(kFull, pwd.x, 1);
+    const double ew = __shfl_down_sync(kFull, pwd.y, 1);
+    const double el = __shfl_down_sync(kFull, pl, 1);
+    if (valid && owner && be > b) {
+      n_eval += (unsigned long long)(be - b);
+      if (COORD == kObs) {
+        add_sums<COORD>(A, d, R, k, 0, be - b, ewd - pwd.x, ew - pwd.y, el - pl, acc);
+      } else if (code == ce) {
+        if (code >= 0 && code < n1) add_sums<COORD>(A, d, R, k, code, be - b, ewd - pwd.x, ew - pwd.y, el - pl, acc);
+      } else {
+        do_run_from<COORD, MINPOS>(A, d, colx, pre, c, R, k, b, be, code, acc, rech);
+      }
     }
   }
-  if (act) {
-    acc_flush8<COORD>(A, d, k, acc.B, acc.s0);
-    acc_flush8<COORD>(A, d, k, acc.B + 1, acc.s1);
-  }
+  if (owner) acc.finish<COORD>(A, d, k);
   stats[0] += n_eval;
   stats[1] += rech;
 }
 
 template <int COORD, bool MINPOS>
-__global__ void __launch_bounds__(kGridWarps * 32, 4) grid_kernel(PairArgs args) {
+__global__ void __launch_bounds__(kGridThreads, 4) grid_kernel(PairArgs args) {
   // the arguments in shared memory: helpers take them by reference without a
   // per-thread local copy of the parameter block
   __shared__ PairArgs A;
+  __shared__ double prev[8 * kGridThreads];  // GridAcc's sums of code C - 1, per lane
   if (threadIdx.x == 0) A = args;
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -125,7 +212,9 @@ __global__ void __launch_bounds__(kGridWarps * 32, 4) grid_kernel(PairArgs args)
     ++n_taken;
     if (it.r_hi <= it.r_lo) continue;
     const int fi = (int)A.gfirst[it.i], fj = (int)A.gfirst[it.j];
-    for (int t0 = 0; t0 < 2 * n0; t0 += 32) grid_group<COORD, MINPOS>(A, it, fi, fj, t0, lane, stats);
+    for (int t0 = 0; t0 < 2 * n0 + 1; t0 += kPassRuns)
+      grid_pass<COORD, MINPOS>(A, it, fi, fj, t0, min(kPassRuns, 2 * n0 + 1 - t0), lane, prev + threadIdx.x,
+                               stats);
   }
   add_counters(A, lane, stats[0], stats[1], n_taken, 9);
 }
@@ -135,9 +224,9 @@ template <int COORD, bool MINPOS>
 cudaError_t launch_grid(const PairArgs& a, int num_sms, cudaStream_t stream) {
   int per_sm = 0;
   const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, grid_kernel<COORD, MINPOS>, kGridWarps * 32, 0);
+      &per_sm, grid_kernel<COORD, MINPOS>, kGridThreads, 0);
   if (e != cudaSuccess) return e;
-  grid_kernel<COORD, MINPOS><<<num_sms * (per_sm > 0 ? per_sm : 1), kGridWarps * 32, 0, stream>>>(a);
+  grid_kernel<COORD, MINPOS><<<num_sms * (per_sm > 0 ? per_sm : 1), kGridThreads, 0, stream>>>(a);
   return cudaGetLastError();
 }
 

@@ -514,12 +514,14 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) pair_kernel(PairArgs A) {
     const double zlo = dmul(dsub(dmul(0.5, (double)lsum_lo), A.g.min2), A.g.invn2);
     const double zhi = dmul(dsub(dmul(0.5, (double)lsum_hi), A.g.min2), A.g.invn2);
     it.zb = zbin_of_sum(lsum_lo, A.g);
-    it.zconst = (zlo > -1.0 && zhi < 2147483648.0 && it.zb == zbin_of_sum(lsum_hi, A.g)) ? 1 : 0;
+    const uint32_t zb_hi = zbin_of_sum(lsum_hi, A.g);
+    it.zconst = (zlo > -1.0 && zhi < 2147483648.0 && it.zb == zb_hi) ? 1 : 0;
     it.lo1 = 0;
     if (A.run_split && run_item(A, it.c, it.zconst)) continue;  // run-sweep kernel's item
-    // with run_split every field uses the wide fixed-point scale, which only
-    // the direct (exact) path supports
-    const bool exact_item = A.force_exact || !it.zconst || A.run_split;
+    if (diag_item(A, zlo, zhi, it.zb, zb_hi)) continue;          // diagonal-sweep kernel's item
+    // with run_split or diag_split every field uses the wide fixed-point
+    // scale, which only the direct (exact) path supports
+    const bool exact_item = A.force_exact || !it.zconst || A.run_split || A.diag_split;
     if (exact_item)
       process_item<COORD, EXACT0, MINPOS, 1>(A, it, win, lane, n_eval, n_recheck);
     else

@@ -103,10 +103,13 @@ struct PairArgs {
   double run_amin;           // Cartesian: smallest 2(1 - cos theta) the run sweep accepts
   const float* thr;          // run sweep: first-axis thresholds T[0..n0]
   // boundary table of the catalogue's common first-axis grid (grid sweep)
-  const uint16_t* gq;        // [2][ng][n0 + 1]: first grid index of bin >= k (side 0, 1)
+  const uint16_t* gq;        // [ng][2 n0 + 2]: a grid row's run boundaries in column order
+                             // (k_grid_table, engine.cu)
   const uint32_t* gfirst;    // per sightline: grid index of pixel 0, or kNoGrid
   int ng;                    // grid values
   int grid_split;            // the grid kernel takes the run items whose sightlines are on the grid
+  int diag_split;            // Polar: the diagonal-sweep kernel takes the items whose z index is
+                             // constant; the pixel-pair kernel evaluates the rest exactly
   int win_w1;                // window width along axis 1 (Cartesian)
   int win_slots;             // slots per warp window
   unsigned long long* acc;   // [n_rows][ntotal][kAccWords] 128-bit fixed point
@@ -139,6 +142,10 @@ size_t pair_kernel_smem(int win_slots);
 // run_item() accepts and whose two sightlines lie on the common grid.
 cudaError_t launch_grid_kernel(const PairArgs& a, int coord, bool minpos, int num_sms,
                                cudaStream_t stream);
+
+// Launch the persistent diagonal-sweep kernel (xi_diag.cu) over the Polar
+// items that diag_item() accepts (every field on the wide scale).
+cudaError_t launch_diag_kernel(const PairArgs& a, bool minpos, int num_sms, cudaStream_t stream);
 
 // Launch the persistent run-sweep kernel (xi_runs.cu) over the items that
 // run_item() accepts: Cartesian and observing coordinates, catalogue sorted

@@ -114,6 +114,8 @@ __device__ __forceinline__ int perp_code(const PairArgs& A, const RowV& R, float
 struct RunAcc {
   int B;
   double s0[8], s1[8];
+  template <int COORD>
+  __device__ __forceinline__ void add(const PairArgs& A, Dest d, int k, int cc, const double (&v)[8]);
 };
 
 // Add one code's sums of first-axis bin k to the per-cell sums (by value, so
@@ -135,23 +137,10 @@ __device__ __forceinline__ void acc_flush8(const PairArgs& A, Dest d, int k, int
   acc_flush<COORD>(A, d, k, c, F);
 }
 
-// Add the sub-run [s, e) with r_perp code cc of first-axis bin k.
+// Add sums v of r_perp code cc to the lane's two FP64 code accumulators.
 template <int COORD>
-__device__ __forceinline__ void add_subrun(const PairArgs& A, Dest d, const double4* pre,
-                                           const RowV& R, int k, int cc, int s, int e,
-                                           RunAcc& acc) {
-  const double4 ps = pre[s], pe = pre[e];
-  const double md = (double)(e - s);
-  const double dwd = pe.x - ps.x, dw = pe.y - ps.y, dl = pe.z - ps.z;
-  double v[8];
-  v[0] = R.wd1 * dwd;
-  v[1] = R.wd1 * md;
-  v[2] = dwd;
-  v[3] = R.w1 * dw;
-  v[4] = R.w1 * md;
-  v[5] = dw;
-  v[6] = __fma_rn(R.hl1, md, 0.5 * dl);
-  v[7] = md;
+__device__ __forceinline__ void add_vals(const PairArgs& A, Dest d, int k, int cc, const double (&v)[8],
+                                         RunAcc& acc) {
   if (acc.B < 0) acc.B = cc;
   if (cc == acc.B) {
 #pragma unroll
@@ -181,18 +170,47 @@ __device__ __forceinline__ void add_subrun(const PairArgs& A, Dest d, const doub
   }
 }
 
-// One run [s, e) of first-axis bin k in row R: split by r_perp code (codes at
-// the run's ends; bisection between them when they differ) and add.
-template <int COORD, bool MINPOS>
-__device__ __forceinline__ void do_run(const PairArgs& A, Dest d, const float* colx,
-                                       const double4* pre, double c, const RowV& R, int k, int s,
-                                       int e, RunAcc& acc, unsigned& rech) {
-  if (COORD == kObs) {
-    add_subrun<COORD>(A, d, pre, R, k, 0, s, e, acc);
-    return;
-  }
-  const int ce = perp_code<MINPOS>(A, R, colx[e - 1], c, rech);
-  int code = (e - 1 == s) ? ce : perp_code<MINPOS>(A, R, colx[s], c, rech);
+template <int COORD>
+__device__ __forceinline__ void RunAcc::add(const PairArgs& A, Dest d, int k, int cc, const double (&v)[8]) {
+  add_vals<COORD>(A, d, k, cc, v, *this);
+}
+
+// Add a sub-run of m columns with r_perp code cc of first-axis bin k, given
+// the differences of sightline j's prefix sums over it (w*delta, w, loglam),
+// to the lane's code accumulators (RunAcc, or the grid sweep's GridAcc).
+template <int COORD, class Acc>
+__device__ __forceinline__ void add_sums(const PairArgs& A, Dest d, const RowV& R, int k, int cc, int m,
+                                         double dwd, double dw, double dl, Acc& acc) {
+  double v[8];
+  const double md = (double)m;
+  v[0] = R.wd1 * dwd;
+  v[1] = R.wd1 * md;
+  v[2] = dwd;
+  v[3] = R.w1 * dw;
+  v[4] = R.w1 * md;
+  v[5] = dw;
+  v[6] = __fma_rn(R.hl1, md, 0.5 * dl);
+  v[7] = md;
+  acc.template add<COORD>(A, d, k, cc, v);
+}
+
+// Add the sub-run [s, e) with r_perp code cc of first-axis bin k.
+template <int COORD, class Acc>
+__device__ __forceinline__ void add_subrun(const PairArgs& A, Dest d, const double4* pre,
+                                           const RowV& R, int k, int cc, int s, int e,
+                                           Acc& acc) {
+  const double4 ps = pre[s], pe = pre[e];
+  add_sums<COORD>(A, d, R, k, cc, e - s, pe.x - ps.x, pe.y - ps.y, pe.z - ps.z, acc);
+}
+
+// One run [s, e) of first-axis bin k in row R whose first column has r_perp
+// code `code`: split by r_perp code (the code at the run's end; bisection
+// between the ends when they differ) and add.
+template <int COORD, bool MINPOS, class Acc>
+__device__ __forceinline__ void do_run_from(const PairArgs& A, Dest d, const float* colx,
+                                            const double4* pre, double c, const RowV& R, int k, int s,
+                                            int e, int code, Acc& acc, unsigned& rech) {
+  const int ce = (e - 1 == s) ? code : perp_code<MINPOS>(A, R, colx[e - 1], c, rech);
   const int n1 = (int)A.g.n1;
   if (code == ce) {  // one r_perp bin over the whole run
     if (code >= 0 && code < n1) add_subrun<COORD>(A, d, pre, R, k, code, s, e, acc);
@@ -220,6 +238,20 @@ __device__ __forceinline__ void do_run(const PairArgs& A, Dest d, const float* c
     start = end;
     code = perp_code<MINPOS>(A, R, colx[end], c, rech);
   }
+}
+
+// One run [s, e) of first-axis bin k in row R: split by r_perp code (codes at
+// the run's ends; bisection between them when they differ) and add.
+template <int COORD, bool MINPOS>
+__device__ __forceinline__ void do_run(const PairArgs& A, Dest d, const float* colx,
+                                       const double4* pre, double c, const RowV& R, int k, int s,
+                                       int e, RunAcc& acc, unsigned& rech) {
+  if (COORD == kObs) {
+    add_subrun<COORD>(A, d, pre, R, k, 0, s, e, acc);
+    return;
+  }
+  const int code = perp_code<MINPOS>(A, R, colx[s], c, rech);
+  do_run_from<COORD, MINPOS, RunAcc>(A, d, colx, pre, c, R, k, s, e, code, acc, rech);
 }
 
 // first p in [lo, n) with pred(col[p]); pred monotone
@@ -293,15 +325,30 @@ __device__ __forceinline__ bool load_item(const PairArgs& A, unsigned long long 
   return true;
 }
 
-// Row r of an item.
+// The loaded values of row r of an item (loaded a row ahead by the grid
+// sweep) and the row values derived from them.
+struct RowRaw {
+  float d1, w1, l1;
+  double wd1;
+};
+
+__device__ __forceinline__ RowRaw row_raw(const float* rowd, const double* rowwd, const float* roww,
+                                          const float* rowl, int r) {
+  RowRaw q;
+  q.d1 = rowd[r];
+  q.wd1 = rowwd[r];
+  q.w1 = roww[r];
+  q.l1 = rowl[r];
+  return q;
+}
+
 template <int COORD>
-__device__ __forceinline__ RowV row_values(const float* rowd, const double* rowwd, const float* roww,
-                                           const float* rowl, float ap, float inv1sqf, int r) {
+__device__ __forceinline__ RowV row_derive(const RowRaw& q, float ap, float inv1sqf) {
   RowV R;
-  R.d1 = rowd[r];
-  R.wd1 = rowwd[r];
-  R.w1 = (double)roww[r];
-  R.hl1 = 0.5 * (double)rowl[r];
+  R.d1 = q.d1;
+  R.wd1 = q.wd1;
+  R.w1 = (double)q.w1;
+  R.hl1 = 0.5 * (double)q.l1;
   if (COORD == kCart) {
     const float p = __fmul_rn(R.d1, R.d1);
     const float err = __fmaf_rn(R.d1, R.d1, -p);  // d1*d1 = p + err exactly
@@ -311,6 +358,13 @@ __device__ __forceinline__ RowV row_values(const float* rowd, const double* roww
     R.A1 = R.dl1 = 0.f;
   }
   return R;
+}
+
+// Row r of an item.
+template <int COORD>
+__device__ __forceinline__ RowV row_values(const float* rowd, const double* rowwd, const float* roww,
+                                           const float* rowl, float ap, float inv1sqf, int r) {
+  return row_derive<COORD>(row_raw(rowd, rowwd, roww, rowl, r), ap, inv1sqf);
 }
 
 // Warp-sum the kernel's counters into A.counters[0] (evaluated pairs), [1]

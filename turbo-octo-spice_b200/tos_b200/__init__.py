@@ -53,7 +53,8 @@ class XiStats(C.Structure):
         "num_pixel_pairs", "num_pixel_pairs_used", "num_pixel_pairs_evaluated", "num_edge_rechecks",
         "num_index_overflow", "num_cells", "num_direct_runs", "num_window_flushes")] + [(n, C.c_double) for n in (
             "max_ang", "cos_max_ang", "ms_expand", "ms_pairs", "ms_total", "ms_device")] + [
-        ("num_run_items", C.c_uint64), ("ms_runs", C.c_double), ("num_grid_items", C.c_uint64), ("ms_grid", C.c_double)]
+        ("num_run_items", C.c_uint64), ("ms_runs", C.c_double), ("num_grid_items", C.c_uint64), ("ms_grid", C.c_double),
+        ("num_diag_items", C.c_uint64), ("ms_diag", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -109,6 +110,7 @@ def lib() -> C.CDLL:
         L.tos_xibin_finalize.restype = None
         L.tos_brute_run.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
         L.tos_brute_run_noalloc.argtypes = [vp, vp, sz, dbl, dbl, i32, vp, vp, vp, C.POINTER(dbl)]
+        L.tos_brute_tune.argtypes = [vp, vp, sz, dbl, dbl, i32, C.POINTER(i32), C.POINTER(i32)]
         L.tos_xi_cell_covariance.argtypes = [vp, vp, vp, vp, vp]
         L.tos_xi_jackknife.argtypes = [vp, vp, i32, sz, C.POINTER(sz), vp, vp, vp]
         L.tos_xi_subsample_covariance.argtypes = [vp, vp, sz, sz, vp, vp, vp]
@@ -129,7 +131,7 @@ def lib() -> C.CDLL:
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
         for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
                      "tos_catalog_sightline_cells", "tos_grid_max_angular_scale", "tos_xi_run",
-                     "tos_brute_run", "tos_comoving_distance", "tos_fill_distances"):
+                     "tos_brute_run", "tos_brute_tune", "tos_comoving_distance", "tos_fill_distances"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -451,6 +453,18 @@ def brute_run(engine: Engine, points: np.ndarray, rmin: float, rmax: float, nbin
     _check(lib().tos_brute_run(engine.handle, _ptr(pts), len(pts), rmin, rmax, nbins, _ptr(dsum), _ptr(wsum),
                                _ptr(counts), C.byref(ms)))
     return dsum, wsum, counts, ms.value
+
+
+def brute_tune(engine: Engine, points: np.ndarray, rmin: float, rmax: float, nbins: int):
+    """tos_brute_tune: time the brute-force kernel's launch shapes on a sample
+    of the points and keep the fastest on the engine for this bin count.
+    Returns (diagonals per lane, warps per CTA) of the pick."""
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    if pts.ndim != 2 or pts.shape[1] != 5:
+        raise ValueError("points must be (n, 5)")
+    k, w = C.c_int(), C.c_int()
+    _check(lib().tos_brute_tune(engine.handle, _ptr(pts), len(pts), rmin, rmax, nbins, C.byref(k), C.byref(w)))
+    return k.value, w.value
 
 
 def brute_run_noalloc(engine: Engine, points_ptr: int, n_points: int, rmin: float, rmax: float,
