@@ -28,6 +28,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "engine_internal.h"
@@ -55,6 +56,7 @@ struct BruteArgs {
   float mag;
   int bits;
   double scale_hi[2];     // 2^(F - 44) of fields dsum, wsum: |run sum| * 2^F < 2^62
+  const double* th;       // [nbins + 3] exact-index thresholds on r^2 (brute_thresholds)
   unsigned long long* acc;       // [nbins + 2][kBWin] 128-bit carry-free sums and counts
   unsigned long long* next;      // diagonal-group counter
   unsigned long long* counters;  // [0] FP64 re-binnings
@@ -82,17 +84,19 @@ __device__ __forceinline__ long long fixed_wide(double c, double sh) {
   return (qh << 44) + ql;
 }
 
-// Histogram index of the FP64 separation: 0 below min, nbins+1 at or above
-// max, else floor((r - min) / spacing) + 1 (gpu/brute.cu:40-48 in FP64).
-__device__ __forceinline__ uint32_t exact_index(const BruteArgs& A, float4 a, float4 b) {
+// Histogram index of the FP64 separation, 0 below min, nbins+1 at or above
+// max, else floor((r - min) / spacing) + 1 with r = sqrt(dx^2 + dy^2 + dz^2)
+// in FP64 (gpu/brute.cu:40-48, bucketxi.cc:79-98).  The index is a
+// non-decreasing function of the FP64 r^2, so th[b] (b = 1 .. nbins + 1) is
+// the smallest r^2 whose index is at least b (brute_thresholds, with
+// th[0] = -1 and th[nbins + 2] = +inf), and an index known to lie within one
+// of `near` is decided by two comparisons of r^2.
+__device__ __forceinline__ uint32_t exact_index(const BruteArgs& A, float4 a, float4 b, int near) {
   const double dx = dsub((double)a.x, (double)b.x), dy = dsub((double)a.y, (double)b.y),
                dz = dsub((double)a.z, (double)b.z);
-  const double r = dsqrt(dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz)));
-  if (r < A.min) return 0u;
-  if (r >= A.max) return (uint32_t)A.nbins + 1u;
-  double k = floor(ddiv(dsub(r, A.min), A.spacing));
-  if (k > (double)(A.nbins - 1)) k = (double)(A.nbins - 1);
-  return (uint32_t)k + 1u;
+  const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+  const int c = min(max(near, 0), A.nbins + 1);
+  return (uint32_t)(c - 1 + (r2 >= A.th[c] ? 1 : 0) + (r2 >= A.th[c + 1] ? 1 : 0));
 }
 
 // Add the queued runs [first, first + cnt) to the warp window, one per lane.
@@ -173,25 +177,32 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
     // columns of row 0: d0 + m (the newest, m = K - 1, is loaded in the loop)
 #pragma unroll
     for (int m = 0; m + 1 < K; ++m) {
-      const int jc = min(d0 + m, A.n - 1);
-      cp[m] = A.pos[jc];
-      cwd[m] = A.wd[jc];
-      cw[m] = A.w[jc];
+      cp[m] = make_float4(0.f, 0.f, 0.f, 0.f);
+      cwd[m] = cw[m] = 0.0;
+      if (d0 + m < A.n) {
+        cp[m] = A.pos[d0 + m];
+        cwd[m] = A.wd[d0 + m];
+        cw[m] = A.w[d0 + m];
+      }
     }
     int qn = 0;  // queued runs (the same in every lane)
+    // the lane's newest column (t + d0 + K - 1) and the row, walked by pointer
+    const float4* pj = A.pos + (d0 + K - 1);
+    const double* wdj = A.wd + (d0 + K - 1);
+    const double* wj = A.w + (d0 + K - 1);
+    const int j_end = A.n - (d0 + K - 1);  // rows t < j_end have the newest column
 #pragma unroll 1
     for (int t = 0; t < t_end; ++t) {
-      {
-        const int jc = min(t + d0 + K - 1, A.n - 1);
-        cp[K - 1] = A.pos[jc];
-        cwd[K - 1] = A.wd[jc];
-        cw[K - 1] = A.w[jc];
+      if (t < j_end) {
+        cp[K - 1] = pj[t];
+        cwd[K - 1] = wdj[t];
+        cw[K - 1] = wj[t];
       }
       const float4 pi = A.pos[t];
       const double wdi = A.wd[t], wi = A.w[t];
 #pragma unroll
       for (int m = 0; m < K; ++m) {
-        const bool in = t + d0 + m < A.n;
+        const bool in = t < j_end + (K - 1 - m);  // t + d0 + m < n
         const float dx = __fsub_rn(pi.x, cp[m].x), dy = __fsub_rn(pi.y, cp[m].y),
                     dz = __fsub_rn(pi.z, cp[m].z);
         const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
@@ -203,7 +214,7 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
         const bool recheck = in && (((qq + 1) & ((1 << A.k) - 1)) < 2) && (tt < A.nbp1f) && (tt > -1.f);
         if (__any_sync(kFull, recheck)) {
           if (recheck) {
-            key = exact_index(A, pi, cp[m]);
+            key = exact_index(A, pi, cp[m], b);
             ++n_recheck;
           }
         }
@@ -326,6 +337,46 @@ void brute_args(BruteArgs& A, int n, int nbins, double min, double max, double m
 
 double brute_inv_scale(const BruteArgs& A, int f) { return 1.0 / (A.scale_hi[f] * 17592186044416.0); }
 
+// The histogram index of an FP64 squared separation r2, computed as the
+// reference's double-precision estimator does from r = sqrt(r2).
+int brute_index_of_r2(double r2, double min, double max, double spacing, int nbins) {
+  const double r = std::sqrt(r2);
+  if (r < min) return 0;
+  if (r >= max) return nbins + 1;
+  double k = std::floor(tos::ddiv(tos::dsub(r, min), spacing));
+  if (k > (double)(nbins - 1)) k = (double)(nbins - 1);
+  return (int)k + 1;
+}
+
+// th[b], b = 1 .. nbins + 1: the smallest double r2 >= 0 whose index is at
+// least b (bisection over the ordered bit patterns of non-negative doubles;
+// the index is non-decreasing in r2), th[0] = -1, th[nbins + 2] = +inf.
+// IEEE sqrt, subtraction and division round the same on the host and the
+// device, so the device's comparisons reproduce the FP64 index exactly.
+std::vector<double> brute_thresholds(double min, double max, int nbins) {
+  std::vector<double> th((size_t)nbins + 3);
+  th[0] = -1.0;
+  th[(size_t)nbins + 2] = std::numeric_limits<double>::infinity();
+  const double spacing = (max - min) / nbins;
+  const uint64_t top = 0x7FF0000000000000ull;  // +inf
+  for (int b = 1; b <= nbins + 1; ++b) {
+    uint64_t lo = 0, hi = top;  // index(lo bits) < b <= index(hi bits) unless lo already reaches b
+    double v;
+    std::memcpy(&v, &lo, 8);
+    if (brute_index_of_r2(v, min, max, spacing, nbins) >= b) {
+      th[b] = 0.0;
+      continue;
+    }
+    while (hi - lo > 1) {
+      const uint64_t mid = lo + (hi - lo) / 2;
+      std::memcpy(&v, &mid, 8);
+      if (brute_index_of_r2(v, min, max, spacing, nbins) >= b) hi = mid; else lo = mid;
+    }
+    std::memcpy(&th[b], &hi, 8);
+  }
+  return th;
+}
+
 // Launch variant `vi` with up to `warps_max` warps per CTA, persistent (as
 // many CTAs as fit on the SMs), between events ev[4] and ev[5].
 tos_status brute_launch_shape(tos_engine* e, const BruteArgs& A, cudaStream_t st, int vi, int warps_max) {
@@ -398,6 +449,10 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
   DevBuf<double> d_wd, d_w, d_out;
   DevBuf<unsigned long long> d_acc, d_misc;
   DevBuf<uint64_t> d_cnt;
+  DevBuf<double> d_th;
+  const std::vector<double> th = brute_thresholds(min, max, nbins);  // kept until the stream sync
+  TOS_TRY(d_th.alloc(th.size()));
+  TOS_CUDA_TRY(cudaMemcpyAsync(d_th.p, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   TOS_TRY(d_pts.alloc((size_t)n * 5));
   TOS_TRY(d_pos.alloc(n));
   TOS_TRY(d_wd.alloc(n));
@@ -417,6 +472,7 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
   A.wd = d_wd.p;
   A.w = d_w.p;
   brute_args(A, n, nbins, min, max, mwd, mw);
+  A.th = d_th.p;
   A.acc = d_acc.p;
   A.next = d_misc.p;
   A.counters = d_misc.p + 1;
@@ -468,8 +524,11 @@ extern "C" tos_status tos_brute_tune(tos_engine* e, const float* points, size_t 
   cudaStream_t st = e->stream;
   DevBuf<float> d_pts;
   DevBuf<float4> d_pos;
-  DevBuf<double> d_wd, d_w;
+  DevBuf<double> d_wd, d_w, d_th;
   DevBuf<unsigned long long> d_acc, d_misc;
+  const std::vector<double> th = brute_thresholds(min, max, nbins);  // kept until the stream sync
+  TOS_TRY(d_th.alloc(th.size()));
+  TOS_CUDA_TRY(cudaMemcpyAsync(d_th.p, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   TOS_TRY(d_pts.alloc((size_t)n * 5));
   TOS_TRY(d_pos.alloc(n));
   TOS_TRY(d_wd.alloc(n));
@@ -484,6 +543,7 @@ extern "C" tos_status tos_brute_tune(tos_engine* e, const float* points, size_t 
   A.wd = d_wd.p;
   A.w = d_w.p;
   brute_args(A, n, nbins, min, max, mwd, mw);
+  A.th = d_th.p;
   A.acc = d_acc.p;
   A.next = d_misc.p;
   A.counters = d_misc.p + 1;
@@ -542,7 +602,8 @@ constexpr size_t kNaPos = 0;                                                  //
 constexpr size_t kNaWd = kNaPos + round256(16 * kNoAllocMaxPoints);           // double[n]
 constexpr size_t kNaW = kNaWd + round256(8 * kNoAllocMaxPoints);              // double[n]
 constexpr size_t kNaAcc = kNaW + round256(8 * kNoAllocMaxPoints);             // u64[nbins + 2][kBWin]
-constexpr size_t kNaMisc = kNaAcc + round256(8 * kBWin * (kNoAllocMaxBins + 2));  // u64[8]
+constexpr size_t kNaTh = kNaAcc + round256(8 * kBWin * (kNoAllocMaxBins + 2));  // double[nbins + 3]
+constexpr size_t kNaMisc = kNaTh + round256(8 * (kNoAllocMaxBins + 3));         // u64[8]
 constexpr size_t kNoAllocBytes = kNaMisc + 256;                               // ~8.5 MB
 
 // The scratch.  Host code must not pass this name to a kernel: on the host
@@ -627,8 +688,11 @@ extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points
   double* wd = (double*)(S + kNaWd);
   double* w = (double*)(S + kNaW);
   unsigned long long* acc = (unsigned long long*)(S + kNaAcc);
+  double* thr = (double*)(S + kNaTh);
   unsigned long long* misc = (unsigned long long*)(S + kNaMisc);  // [0] group counter [1] rechecks
                                                                    // [2,3] bounds [4] non-finite
+  const std::vector<double> th = brute_thresholds(min, max, nbins);  // kept until the stream sync
+  TOS_CUDA_TRY(cudaMemcpyAsync(thr, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   // the scratch keeps the previous call's contents: clear what accumulates
   TOS_CUDA_TRY(cudaMemsetAsync(acc, 0, (size_t)nb2 * kBWin * sizeof(unsigned long long), st));
   TOS_CUDA_TRY(cudaMemsetAsync(misc, 0, 8 * sizeof(unsigned long long), st));
@@ -650,6 +714,7 @@ extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points
   A.wd = wd;
   A.w = w;
   brute_args(A, n, nbins, min, max, mwd, mw);
+  A.th = thr;
   A.acc = acc;
   A.next = misc;
   A.counters = misc + 1;

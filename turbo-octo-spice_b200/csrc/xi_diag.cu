@@ -92,18 +92,20 @@ struct DItem {
   const double4* prej;
 };
 
-// Add the run [s0, s1) of diagonal delta with key `key` to the item's cell.
-__device__ __noinline__ void emit_diag(const PairArgs& A, const DItem& it, uint32_t key, int s0, int s1,
-                                       int delta, double didj, double wgt) {
+// Add the run [s0, s1) of diagonal delta with key `key` to row `cell`
+// (z index zb; prefix sums prei, prej of the item's two sightlines).
+__device__ __noinline__ void emit_diag(const PairArgs& A, uint32_t cell, uint32_t zb, const double4* prei,
+                                       const double4* prej, uint32_t key, int s0, int s1, int delta,
+                                       double didj, double wgt) {
   const uint32_t b0 = key >> 16, b1 = key & 0xFFFFu;
-  const uint32_t idx = it.zb + (b1 + b0 * A.g.n1) * A.g.n2;  // as XiEstimator.cc:196-201
+  const uint32_t idx = zb + (b1 + b0 * A.g.n1) * A.g.n2;  // as XiEstimator.cc:196-201
   const unsigned long long m = (unsigned long long)(s1 - s0);
   if (idx >= A.g.ntotal) {
     atomicAdd(&A.counters[2], m);
     return;
   }
-  const double4 ia = it.prei[s0], ib = it.prei[s1];
-  const double4 ja = it.prej[s0 + delta], jb = it.prej[s1 + delta];
+  const double4 ia = prei[s0], ib = prei[s1];
+  const double4 ja = prej[s0 + delta], jb = prej[s1 + delta];
   double v[7];
   v[0] = didj;
   v[1] = ib.x - ia.x;
@@ -112,7 +114,7 @@ __device__ __noinline__ void emit_diag(const PairArgs& A, const DItem& it, uint3
   v[4] = ib.y - ia.y;
   v[5] = jb.y - ja.y;
   v[6] = 0.5 * ((ib.z - ia.z) + (jb.z - ja.z));
-  unsigned long long* base = A.acc + ((size_t)it.cell * A.g.ntotal + idx) * kAccWords;
+  unsigned long long* base = A.acc + ((size_t)cell * A.g.ntotal + idx) * kAccWords;
 #pragma unroll
   for (int f = 0; f < 7; ++f) add128(base + f, base + 7 + f, to_fixed_wide(v[f], A.scale_hi[f]));
   red_add(base + 14, m);
@@ -132,7 +134,7 @@ __device__ __forceinline__ void drain(const PairArgs& A, const DItem& it, const 
   __syncwarp();
   if (lane < n) {
     const DRun r = q[first + lane];
-    emit_diag(A, it, r.key, r.s0, r.s1, r.delta, r.didj, r.wgt);
+    emit_diag(A, it.cell, it.zb, it.prei, it.prej, r.key, r.s0, r.s1, r.delta, r.didj, r.wgt);
   }
   __syncwarp();
 }
@@ -142,8 +144,8 @@ __device__ __forceinline__ void drain(const PairArgs& A, const DItem& it, const 
 // different rows, so a closed run goes to the warp's queue in shared memory
 // and the warp emits 32 of them at a time, one per lane.
 template <bool MINPOS>
-__device__ __noinline__ void diag_group(const PairArgs& A, const DItem& it, int delta0, int dhi, int lane,
-                                        DRun* q, unsigned long long* stats) {
+__device__ __forceinline__ void diag_group(const PairArgs& A, const DItem& it, int delta0, int dhi, int lane,
+                                           DRun* q, unsigned long long* stats) {
   const int delta = delta0 + lane;
   const bool lane_on = delta <= dhi;
   const int s_lo = max(0, -(delta0 + 31));
@@ -157,16 +159,17 @@ __device__ __noinline__ void diag_group(const PairArgs& A, const DItem& it, int 
   unsigned long long n_eval = 0;
 #pragma unroll 1
   for (int s = s_lo; s < s_hi; ++s) {
+    // p2 stays within the 32 sentinels on either side of the padded
+    // distances: p2 >= s_lo + delta0 >= -31 and p2 < s_hi + delta0 + 32 <= nj + 32
     const int p2 = s + delta;
-    const bool in = lane_on && p2 >= 0 && p2 < it.nj;
-    const int pc = min(max(p2, 0), it.nj - 1);
+    const bool in = lane_on && (unsigned)p2 < (unsigned)it.nj;
     DRow R;
     R.d1 = it.rowd[s];
     R.x1 = R.d1;
     const float p = __fmul_rn(R.d1, R.d1);
     R.dl1 = -__fmaf_rn(R.d1, R.d1, -p);  // -(d1*d1 - fl(d1*d1)), exact
     R.A1 = __fmul_rn(R.d1, it.ap);
-    const float x2 = it.cold[pc];
+    const float x2 = it.cold[p2];
     bool recheck;
     uint32_t key = polar_key<MINPOS>(A, R, x2, recheck);
     recheck = recheck && in;
@@ -196,9 +199,9 @@ __device__ __noinline__ void diag_group(const PairArgs& A, const DItem& it, int 
       didj = 0.0;
       wgt = 0.0;
     }
-    if (key != kInvalidKey) {
-      didj = __fma_rn(it.rowwd[s], it.colwd[pc], didj);
-      wgt = __fma_rn((double)it.roww[s], (double)it.colw[pc], wgt);
+    if (key != kInvalidKey) {  // binned: p2 is a pixel of sightline j
+      didj = __fma_rn(it.rowwd[s], it.colwd[p2], didj);
+      wgt = __fma_rn((double)it.roww[s], (double)it.colw[p2], wgt);
     }
   }
   // runs still open at the last row, then the queue
@@ -215,12 +218,12 @@ __device__ __noinline__ void diag_group(const PairArgs& A, const DItem& it, int 
   stats[1] += rech;
 }
 
+// The arguments stay in the kernel's parameter space (__grid_constant__):
+// the inlined sweep reads them as constant-bank operands, and emit_diag
+// takes them by reference without a copy.
 template <bool MINPOS>
-__global__ void __launch_bounds__(kDiagWarps * 32) diag_kernel(PairArgs args) {
-  __shared__ PairArgs A;
+__global__ void __launch_bounds__(kDiagWarps * 32, 3) diag_kernel(const __grid_constant__ PairArgs A) {
   __shared__ DRun queue[kDiagWarps][kQueue];
-  if (threadIdx.x == 0) A = args;
-  __syncthreads();
   const int lane = threadIdx.x & 31;
   DRun* q = queue[threadIdx.x >> 5];
   unsigned long long stats[2] = {0ull, 0ull};  // evaluated pairs, FP64 re-evaluations

@@ -100,8 +100,8 @@ struct GridAcc {
 // moves slowly from row to row) and adds them to the per-cell sums when its
 // codes move on.
 template <int COORD, bool MINPOS>
-__device__ __noinline__ void grid_pass(const PairArgs& A, const SweepItem& it, int fi, int fj, int t0,
-                                       int m, int lane, double* prev, unsigned long long* stats) {
+__device__ __forceinline__ void grid_pass(const PairArgs& A, const SweepItem& it, int fi, int fj, int t0,
+                                          int m, int lane, double* prev, unsigned long long* stats) {
   const int n0 = (int)A.g.n0;
   const int nbd = 2 * n0 + 2;  // boundaries per table row
   const int P = 32 / (m + 1);
@@ -148,25 +148,33 @@ __device__ __noinline__ void grid_pass(const PairArgs& A, const SweepItem& it, i
   const int n1 = (int)A.g.n1;
   const int iters = (g_hi - g_lo + P - 1) / P;  // the same for every phase (shuffles below)
   const uint16_t* tcol = tab + t;
+  auto bound = [&](int row) { return min(max((int)tcol[(size_t)row * nbd] - fj, 0), nj); };
+  // Software pipeline: the boundary of the row after next, and the column
+  // value and prefix sums at the next row's boundary, load while this row is
+  // evaluated (the column data depends on a boundary that is itself a load).
   int r = g_lo + phase;
-  // the next row's boundary and row values, loaded a row ahead
-  int r0 = min(r, g_hi - 1);
-  int nb = min(max((int)tcol[(size_t)r0 * nbd] - fj, 0), nj);
-  RowRaw nR = row_raw(rowd, rowwd, roww, rowl, r0);
+  const int r0 = min(r, g_hi - 1), r1 = min(r + P, g_hi - 1);
+  int b = bound(r0), nb = bound(r1);
+  float x2 = colx[min(b, nj - 1)];
+  double2 pwd = *reinterpret_cast<const double2*>(&pre[b]);
+  double pl = pre[b].z;
+  RowRaw cR = row_raw(rowd, rowwd, roww, rowl, r0);
+  RowRaw nR = row_raw(rowd, rowwd, roww, rowl, r1);
 #pragma unroll 1
   for (int q = 0; q < iters; ++q, r += P) {
     const bool valid = act && r < g_hi;
-    const int b = nb;
-    const RowV R = row_derive<COORD>(nR, ap, inv1sqf);
-    const int rn = min(r + P, g_hi - 1);
-    nb = min(max((int)tcol[(size_t)rn * nbd] - fj, 0), nj);
-    nR = row_raw(rowd, rowwd, roww, rowl, rn);
+    // loads for the rows ahead
+    const float nx2 = colx[min(nb, nj - 1)];
+    const double2 npwd = *reinterpret_cast<const double2*>(&pre[nb]);
+    const double npl = pre[nb].z;
+    const int r2 = min(r + 2 * P, g_hi - 1);
+    const int nnb = bound(r2);
+    const RowRaw nnR = row_raw(rowd, rowwd, roww, rowl, r2);
+    const RowV R = row_derive<COORD>(cR, ap, inv1sqf);
     // this lane's boundary: r_perp code of column b (of the last column when
     // b = nj: then it is the code of the last column of the run ending here)
     int code = 0;
-    if (COORD == kCart && valid) code = perp_code<MINPOS>(A, R, colx[min(b, nj - 1)], c, rech);
-    const double2 pwd = *reinterpret_cast<const double2*>(&pre[b]);
-    const double pl = pre[b].z;
+    if (COORD == kCart && valid) code = perp_code<MINPOS>(A, R, x2, c, rech);
     const int be = __shfl_down_sync(kFull, b, 1);
     const int ce = __shfl_down_sync(kFull, code, 1);
     const double ewd = __shfl_down_sync(kFull, pwd.x, 1);
@@ -182,20 +190,25 @@ __device__ __noinline__ void grid_pass(const PairArgs& A, const SweepItem& it, i
         do_run_from<COORD, MINPOS>(A, d, colx, pre, c, R, k, b, be, code, acc, rech);
       }
     }
+    b = nb;
+    nb = nnb;
+    x2 = nx2;
+    pwd = npwd;
+    pl = npl;
+    cR = nR;
+    nR = nnR;
   }
   if (owner) acc.finish<COORD>(A, d, k);
   stats[0] += n_eval;
   stats[1] += rech;
 }
 
+// The arguments stay in the kernel's parameter space (__grid_constant__):
+// the inlined sweep reads them as constant-bank operands, and the rarely
+// called out-of-line helpers take them by reference without a copy.
 template <int COORD, bool MINPOS>
-__global__ void __launch_bounds__(kGridThreads, 4) grid_kernel(PairArgs args) {
-  // the arguments in shared memory: helpers take them by reference without a
-  // per-thread local copy of the parameter block
-  __shared__ PairArgs A;
+__global__ void __launch_bounds__(kGridThreads, 4) grid_kernel(const __grid_constant__ PairArgs A) {
   __shared__ double prev[8 * kGridThreads];  // GridAcc's sums of code C - 1, per lane
-  if (threadIdx.x == 0) A = args;
-  __syncthreads();
   const int lane = threadIdx.x & 31;
   unsigned long long stats[2] = {0ull, 0ull};  // evaluated pairs, FP64 re-evaluations
   unsigned long long n_taken = 0;
