@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["full", "small", "brute"], default="full")
+    ap.add_argument("--workload", choices=["full", "small", "brute", "serving"], default="full")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-cells", type=int, default=40,
                     help="CPU legs: primary cells of the seeded sample the reference path is timed on")
@@ -72,8 +72,14 @@ def parse():
                     help="full workload: sightlines over the same ~10000 deg^2 (profiling uses fewer)")
     ap.add_argument("--grid", choices=["cartesian", "polar"], default="cartesian",
                     help="binning of the plain workloads: (r_par,r_perp) 50x50 or (r,mu) 50x20")
-    ap.add_argument("--mocks", type=int, default=2,
-                    help="batched sample: the first M mocks of the seeded 256-mock draw (0: skip)")
+    ap.add_argument("--mocks", type=int, default=32,
+                    help="batched sample: M mocks of the seeded 256-mock draw (0: skip)")
+    ap.add_argument("--mock-sample", choices=["stratified", "first"], default="stratified",
+                    help="batched sample: every (256/M)-th mock by size from the smallest, or the first M")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the launch-shape autotuner in the first warm-up step")
+    ap.add_argument("--no-polar", action="store_true",
+                    help="skip the (r,mu) 50x20 count of the full workload's catalogue")
     ap.add_argument("--no-jackknife", action="store_true",
                     help="skip the one-pass jackknife of the full-survey catalogue")
     ap.add_argument("--requests", type=int, default=12,
@@ -387,8 +393,12 @@ def engine_arm(args, D):
     dev = D.local
     eng = T.Engine(dev)
     ops = OPS_PER_PAIR[W["ops"]]
+    tuned = None
     if "pts" in W:
         pts = W["pts"]
+        if not args.no_tune:
+            k, wp = T.brute_tune(eng, pts, 0.0, 200.0, 100)
+            tuned = {"diagonals_per_lane": k, "warps_per_cta": wp}
         for _ in range(args.warmup):
             T.brute_run(eng, pts, 0.0, 200.0, 100)
         D.barrier()
@@ -418,8 +428,8 @@ def engine_arm(args, D):
             par = brute_parity(eng, pts)
     else:
         cat = T.Catalog(eng, W["los"], W["px"], W["order"])
-        for _ in range(args.warmup):
-            T.xi_run(eng, cat, W["grid"], W["scale"])
+        for w in range(args.warmup):
+            T.xi_run(eng, cat, W["grid"], W["scale"], tune=(w == 0 and not args.no_tune))
         torch.cuda.synchronize(dev)
         D.barrier()
         clk = ClockSampler(dev)
@@ -444,11 +454,15 @@ def engine_arm(args, D):
                        "pair_kernel" if st["num_run_items"] == 0 else "grid/run/pair kernels")
         evaluated = int(st["num_pixel_pairs_evaluated"])
         launches = LAUNCHES_PER_RUN * args.steps
-        jk = par = None
+        jk = par = pol = None
+        if not args.no_tune:
+            tuned = {"ctas_per_sm": "picked by TOS_XI_TUNE in the first warm-up step"}
         if D.rank == 0 and D.world == 1 and not args.no_parity:
             par = parity_measure(eng, cat, W, bins)
         if D.rank == 0 and D.world == 1 and not args.no_jackknife:
             jk = jackknife_measure(eng, cat, W, ms_max / args.steps / 1e3, bins)
+        if D.rank == 0 and D.world == 1 and not args.no_polar and args.grid == "cartesian":
+            pol = polar_measure(eng, cat, W, args)
         cat.close()
         # end to end through the public API from pinned host buffers
         _tl, los_p = pinned_copy(W["los"])
@@ -498,12 +512,16 @@ def engine_arm(args, D):
         line["ms_expand"] = st["ms_expand"]
     if par is not None:
         line["parity"] = par
+    if tuned is not None:
+        line["launch_shape"] = tuned
     if D.rank == 0 and D.world == 1 and "pts" not in W:
         if jk is not None:
             line["jackknife"] = jk
+        if pol is not None:
+            line["polar"] = pol
         if args.mocks > 0:
             t = time.perf_counter()
-            line["batched"] = batched_measure(eng, args.mocks, 1)
+            line["batched"] = batched_measure(eng, args.mocks, 1, args.mock_sample)
             line["batched"]["section_wall_s"] = time.perf_counter() - t
         if args.requests > 0:
             t = time.perf_counter()
@@ -516,6 +534,29 @@ def engine_arm(args, D):
     if D.rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
+
+
+def polar_measure(eng, cat, W, args):
+    """The same catalogue in (r, mu) 50x20 bins to 200 Mpc/h (the binning of
+    the batched and serving configurations): one tuned warm-up, one timed
+    count, and the checker leg on 24 primary cells as for the main line."""
+    import tos_b200 as T
+    g = T.Grid.polar("[0:200]*50", "[0:1]*20")
+    T.xi_run(eng, cat, g, W["scale"], tune=not args.no_tune)
+    bins, _, st = T.xi_run(eng, cat, g, W["scale"])
+    pairs = int(st["num_pixel_pairs"])
+    sec = st["ms_device"] / 1e3
+    out = {"workload": W["config"]["workload"].replace("(r_par,r_perp) 50x50", "(r,mu) 50x20"),
+           "value": pairs / sec, "unit": UNIT, "ms_per_step": st["ms_device"],
+           "kernel": "diag_kernel", "kernel_ms": st["ms_diag"],
+           "diag_sightline_pairs": int(st["num_diag_items"]),
+           "sightline_pairs": int(st["num_sightline_pairs_used"])}
+    peak = NSM * FP32_LANES_PER_SM * 1965.0 * 1e6
+    out["roofline_frac"] = pairs * OPS_PER_PAIR["polar"] / (st["ms_diag"] / 1e3) / peak
+    if not args.no_parity:
+        Wp = dict(W, grid=g)
+        out["parity"] = parity_measure(eng, cat, Wp, bins)
+    return out
 
 
 # ---------------------------------------------------------------- batched and served
@@ -531,25 +572,30 @@ def reduced(los, px, keep):
     return r_los, np.concatenate(chunks)
 
 
-def batched_measure(eng, n_mocks, reps):
-    """Plain vs batched on a bounded sample of the batched configuration: the
-    first M mocks of the seeded 256-mock draw (sightline counts log-uniform in
-    [2k, 40k], each on its own cap at 16 per deg^2), (r, mu) 50x20 bins to
-    200 Mpc/h.  plain = one catalogue and one pair count per mock, one after
+def batched_measure(eng, n_mocks, reps, sample="stratified"):
+    """Plain vs batched on a sample of the batched configuration: M of the
+    seeded 256 mocks (sightline counts log-uniform in [2k, 40k], each on its
+    own cap at 16 per deg^2), either every (256/M)-th by size from the
+    smallest (stratified) or the first M, (r, mu) 50x20 bins to 200 Mpc/h.  plain = one catalogue and one pair count per mock, one after
     another; batched = one catalogue holding every mock as a sightline group
     and one TOS_XI_PER_GROUP count.  Both wall-clock, catalogues resident.
     Jackknife: every (mock, HEALPix nside=8 region) subsample in one pass,
     against separate runs on reduced catalogues (a few timed, scaled to all)."""
     import tos_b200 as T
     from tos_b200 import synth
-    parts, scale = synth.mock_batch(n_mocks=n_mocks, seed=11)
+    if sample == "stratified":
+        parts, scale, picked = synth.mock_batch_stratified(n_pick=n_mocks, seed=11)
+        sample_desc = (f"{len(parts)} of the seeded 256-mock draw, every {256 // max(1, n_mocks)}-th by "
+                       "sightline count from the smallest")
+    else:
+        parts, scale = synth.mock_batch(n_mocks=n_mocks, seed=11)
+        sample_desc = f"first {len(parts)} mocks of the seeded 256-mock draw"
     g = T.Grid.polar("[0:200]*50", "[0:1]*20")
     los, px = synth.merge_groups(parts)
     bcat = T.Catalog(eng, los, px, 6)
     cats = [T.Catalog(eng, l, p, 6) for l, p in parts]
-    T.xi_run(eng, bcat, g, scale, per_group=True)  # warm-up
-    for c in cats:
-        T.xi_run(eng, c, g, scale)
+    T.xi_run(eng, bcat, g, scale, per_group=True)  # warm-up (the kernels are warm from the main line)
+    T.xi_run(eng, cats[0], g, scale)
     t_b, t_p = [], []
     for _ in range(reps):
         t = time.perf_counter()
@@ -585,8 +631,9 @@ def batched_measure(eng, n_mocks, reps):
     for c in cats:
         c.close()
     sep = float(np.mean(times))
-    return {"workload": f"first {len(parts)} mocks of the seeded 256-mock draw (counts log-uniform "
-                        "[2k,40k], own cap each at 16/deg^2), (r,mu) 50x20 bins to 200 Mpc/h, nside=64 cells",
+    return {"workload": sample_desc + " (counts log-uniform [2k,40k], own cap each at 16/deg^2), "
+                        "(r,mu) 50x20 bins to 200 Mpc/h, nside=64 cells",
+            "mock_sightlines_min_max": [int(min(len(p[0]) for p in parts)), int(max(len(p[0]) for p in parts))],
             "mocks": len(parts), "sightlines": int(len(los)), "pixels": int(len(px)), "pixel_pairs": pairs,
             "plain": {"value": pairs / tp, "unit": UNIT, "wall_s": tp,
                       "how": "one catalogue and one tos_xi_run per mock, in turn"},
@@ -657,9 +704,10 @@ def serving_measure(W, n_requests, serve_max,
     grids = [T.Grid.cartesian(), T.Grid.polar("[0:200]*50", "[0:1]*20")]
     gpick = rng.integers(0, 2, n_requests)
     los, px = W["los"], W["px"]
+    cap = "" if serve_max >= 160000 else f" capped at {serve_max} to bound the bench's time"
     out = {"workload": "pool of 6 resident catalogues (first N sightlines of the full survey, N log-uniform "
-                       f"[1k,160k] capped at {serve_max}), Poisson arrivals at 20/s, binning (r_par,r_perp) "
-                       "50x50 or (r,mu) 50x20 at random, 150 GB budget, FIFO admission",
+                       f"[1k,160k]{cap}), {n_requests} Poisson arrivals at 20/s, binning (r_par,r_perp) "
+                       "50x50 or (r,mu) 50x20 at random, 150 GB budget",
            "pool_sightlines": [int(c) for c in counts], "requests": int(n_requests)}
     for policy, slots in runs:
         srv = T.Server(0, slots=slots, memory_budget_bytes=150 * 10**9)
@@ -707,12 +755,32 @@ def serving_measure(W, n_requests, serve_max,
     return out
 
 
+def serving_arm(args, D):
+    """--workload serving: the serving configuration at its own shape, on
+    rank 0: Poisson arrivals at 20/s of --requests requests (default 60) over
+    a resident pool of catalogues whose sightline counts are log-uniform in
+    [1k, 160k] (no cap), with 4 slots (FIFO and shortest-first) and with one."""
+    if D.rank != 0:
+        return
+    W = make_workload("full", args.sightlines, "cartesian")
+    n_req = args.requests if args.requests != 12 else 60
+    out = serving_measure(W, n_req, 160000, runs=(("fifo", 4), ("shortest", 4), ("fifo", 1)))
+    best = out["fifo_slots_4"]
+    line = {"metric": METRIC, "value": best["value"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": best["makespan_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "serving: " + out["workload"]}, "serving": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     D = Dist(args.gpus)
     try:
         if args.impl == "reference":
             reference_arm(args, D)
+        elif args.workload == "serving":
+            serving_arm(args, D)
         else:
             engine_arm(args, D)
     finally:

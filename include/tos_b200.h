@@ -172,6 +172,11 @@ tos_status tos_catalog_groups(const tos_catalog* catalog, uint32_t* group_ids, s
 #define TOS_XI_SUBSAMPLES 0x1u   /* also return per-cell sums (skybin_xis_) */
 #define TOS_XI_EXACT      0x2u   /* evaluate every pixel pair in FP64 (validation path, slow) */
 #define TOS_XI_PER_GROUP  0x4u   /* return per-group sums: one xi per catalogue of a batch */
+#define TOS_XI_TUNE       0x8u   /* autotune first: time the dominant kernel (grid or diagonal
+                                  * sweep) with 1 .. max CTAs per SM on the first 65,536
+                                  * sightline pairs, keep the fastest on the engine for this
+                                  * coordinate type and bin count (later calls use it); the
+                                  * results do not depend on the pick */
 
 /* Maximum angular scale of a grid for a transverse comoving scale:
  * CartesianGrid::maxAngularScale (CartesianGrid.h:45-46),

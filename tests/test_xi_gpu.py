@@ -259,3 +259,21 @@ def test_pointer_sweep_on_gapped_sightlines(engine, name):
     # both sweeps ran: grid pairs and pairs with a gapped sightline
     assert 0 < st["num_grid_items"] < st["num_run_items"]
     assert st["num_run_items"] == st["num_sightline_pairs_used"]
+
+
+@pytest.mark.parametrize("name", ["cartesian", "polar", "observing"])
+def test_tuned_launch_shape_gives_identical_results(engine, name):
+    """TOS_XI_TUNE times the dominant kernel with every CTA count per SM on
+    a sample of the sightline pairs and keeps the fastest on the engine.  A
+    warp sweeps an item on its own and every add is an integer add, so the
+    tuning run and the runs after it give the untuned results bit for bit."""
+    los, px, meta = small_catalog(n=300, seed=21, size_deg=4.0)
+    g = GRIDS[name]
+    cat = T.Catalog(engine, los, px, 6)
+    a, ac, _ = T.xi_run(engine, cat, g, meta["scale"], subsamples=True)
+    b, bc, st = T.xi_run(engine, cat, g, meta["scale"], subsamples=True, tune=True)
+    c, cc, _ = T.xi_run(engine, cat, g, meta["scale"], subsamples=True)
+    cat.close()
+    assert st["num_grid_items"] + st["num_diag_items"] > 0.9 * st["num_sightline_pairs_used"]
+    for x, y in ((a, b), (ac, bc), (a, c), (ac, cc)):
+        assert np.array_equal(x, y)

@@ -924,6 +924,14 @@ size_t Workspace::bytes() const {
          d_counters.bytes() + d_thr.bytes() + d_gq.bytes() + d_cub_tmp.bytes();
 }
 
+// Counter words of a run: kernel counters [0, 16), the theta-edge flags of
+// observing grids from 16 (at most 1 + 4096), then one item counter per
+// chunk of a shared-GPU sweep.
+constexpr int kChunkCounters = 4128;
+constexpr int kMaxChunks = 64;
+constexpr uint64_t kChunkItemsMin = 131072;  // tens of ms per chunk: the launch tail stays small
+constexpr size_t kCounterWords = kChunkCounters + kMaxChunks;
+
 // Fixed-point scales for kernels whose FP64 register sums can hold a whole
 // item's pairs of a bin (at most max_np^2 pairs): every field takes the wide
 // 62-bit conversion (the run, grid and diagonal sweeps).
@@ -943,7 +951,7 @@ static void set_wide_scales(PairArgs& A, const tos_catalog* cat) {
 
 tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos_grid* grid,
                        double scale, uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
-                       tos_xibin* out_cells, tos_xi_stats* stats) {
+                       tos_xibin* out_cells, tos_xi_stats* stats, const SweepShare* share) {
   const auto t_start = std::chrono::steady_clock::now();
   if (!e || !cat || !ws || !out_bins) return fail(TOS_ERR_INVALID_ARG, "null argument");
   if (cat->device != e->device) return fail(TOS_ERR_INVALID_ARG, "catalogue is on another device");
@@ -1007,9 +1015,9 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
   TOS_TRY(ws->d_cand.alloc(nm));
   TOS_TRY(ws->d_item_off.alloc(nm));
   TOS_TRY(ws->d_cell_pairs.alloc(nc));
-  TOS_TRY(ws->d_counters.alloc(4200));
+  TOS_TRY(ws->d_counters.alloc(kCounterWords));
   TOS_CUDA_TRY(cudaMemsetAsync(ws->d_cell_pairs.p, 0, nc * 8, st));
-  TOS_CUDA_TRY(cudaMemsetAsync(ws->d_counters.p, 0, 4200 * 8, st));
+  TOS_CUDA_TRY(cudaMemsetAsync(ws->d_counters.p, 0, kCounterWords * 8, st));
   // [0..3] kernel counters, [4] pair-kernel item counter, [5] candidates,
   // [6] window flushes, [7] run-kernel item counter, [8] run items, [9] grid
   // items, [10] grid-kernel item counter,
@@ -1296,23 +1304,116 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
       use_diag = true;
     }
   }
+  // --- launch shape of the dominant kernel: the tuned CTAs per SM for this
+  // coordinate type and bin count (0: as many as fit).  With TOS_XI_TUNE,
+  // first time every count from 1 to the occupancy limit on the first
+  // kTuneItems sightline pairs (after a warm-up launch), keep the fastest,
+  // and clear what the trials added.  The sums do not depend on the shape: a
+  // warp sweeps an item on its own and every add is an integer add.
+  int ctas_per_sm = 0;
+  const std::pair<int, int> tune_key(G.type, (int)nb);
+  {
+    std::lock_guard<std::mutex> lk(e->tune_mu);
+    auto it = e->xi_tuned.find(tune_key);
+    if (it != e->xi_tuned.end()) ctas_per_sm = it->second;
+  }
+  if ((flags & TOS_XI_TUNE) && (use_grid || use_diag) && n_items > 0) {
+    constexpr uint64_t kTuneItems = 65536;
+    auto trial = [&](int per_sm, int* max_out) -> cudaError_t {
+      PairArgs R = A;
+      R.n_items = std::min<uint64_t>(n_items, kTuneItems);
+      R.next_item = ctr + (use_diag ? 11 : 10);
+      return use_diag ? launch_diag_kernel(R, minpos, e->num_sms, per_sm, st, max_out)
+                      : launch_grid_kernel(R, G.type, minpos, e->num_sms, per_sm, st, max_out);
+    };
+    int max_per_sm = 1;
+    const cudaError_t qe = trial(0, &max_per_sm);
+    if (qe != cudaSuccess) return fail(TOS_ERR_CUDA, std::string("tuning: ") + cudaGetErrorString(qe));
+    float best = 0.f;
+    int pick = max_per_sm;
+    for (int p = 0; p <= max_per_sm; ++p) {  // p = 0: warm-up at the occupancy limit
+      TOS_CUDA_TRY(cudaMemsetAsync(ctr + (use_diag ? 11 : 10), 0, 8, st));
+      TOS_CUDA_TRY(cudaEventRecord(e->ev[4], st));
+      const cudaError_t te = trial(p == 0 ? max_per_sm : p, nullptr);
+      if (te != cudaSuccess) return fail(TOS_ERR_CUDA, std::string("tuning: ") + cudaGetErrorString(te));
+      TOS_CUDA_TRY(cudaEventRecord(e->ev[5], st));
+      TOS_CUDA_TRY(cudaEventSynchronize(e->ev[5]));
+      float ms = 0.f;
+      TOS_CUDA_TRY(cudaEventElapsedTime(&ms, e->ev[4], e->ev[5]));
+      if (p > 0 && (best == 0.f || ms < best)) {
+        best = ms;
+        pick = p;
+      }
+    }
+    ctas_per_sm = pick;
+    {
+      std::lock_guard<std::mutex> lk(e->tune_mu);
+      e->xi_tuned[tune_key] = pick;
+    }
+    TOS_CUDA_TRY(cudaMemsetAsync(ws->d_acc.p, 0, acc_words * 8, st));
+    TOS_CUDA_TRY(cudaMemsetAsync(ctr, 0, 4 * 8, st));          // evaluated, rechecks, overflow, direct
+    TOS_CUDA_TRY(cudaMemsetAsync(ctr + 6, 0, 7 * 8, st));      // flushes, item counters, taken
+  }
+  // Dominant kernel (grid or diagonal sweep): one persistent launch, or for
+  // a shared GPU (SweepShare) a chain of chunk launches, each with its own
+  // item counter (ctr[kChunkCounters + k], after the theta-edge flags of
+  // observing grids at ctr[16 ..]) and its CTA count asked just before launch.
+  auto sweep = [&](bool diag, unsigned long long* counter) -> tos_status {
+    auto launch = [&](const PairArgs& R, int per_sm) -> cudaError_t {
+      return diag ? launch_diag_kernel(R, minpos, e->num_sms, per_sm, st)
+                  : launch_grid_kernel(R, G.type, minpos, e->num_sms, per_sm, st);
+    };
+    if (!share) {
+      PairArgs R = A;
+      R.next_item = counter;
+      const cudaError_t ke = launch(R, ctas_per_sm);
+      if (ke != cudaSuccess)
+        return fail(TOS_ERR_CUDA, std::string(diag ? "diagonal" : "grid") + " kernel: " + cudaGetErrorString(ke));
+      return TOS_OK;
+    }
+    int limit = 1;
+    {
+      PairArgs R = A;
+      const cudaError_t qe = diag ? launch_diag_kernel(R, minpos, e->num_sms, 0, st, &limit)
+                                  : launch_grid_kernel(R, G.type, minpos, e->num_sms, 0, st, &limit);
+      if (qe != cudaSuccess) return fail(TOS_ERR_CUDA, std::string("sweep shape: ") + cudaGetErrorString(qe));
+    }
+    const uint64_t chunks = std::max<uint64_t>(
+        1, std::min<uint64_t>((uint64_t)std::min(std::max(1, share->chunks), kMaxChunks), n_items / kChunkItemsMin));
+    const uint64_t per = (n_items + chunks - 1) / chunks;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    for (auto& ev : done) TOS_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    struct Free {
+      cudaEvent_t* ev;
+      ~Free() {
+        for (int k = 0; k < 2; ++k)
+          if (ev[k]) cudaEventDestroy(ev[k]);
+      }
+    } free_events{done};
+    for (uint64_t c = 0; c < chunks; ++c) {
+      const uint64_t a = c * per, b = std::min<uint64_t>(n_items, a + per);
+      if (a >= b) break;
+      if (c >= 2) TOS_CUDA_TRY(cudaEventSynchronize(done[c % 2]));  // at most two chunks in flight
+      PairArgs R = A;
+      R.item_i = A.item_i + a;
+      R.item_j = A.item_j + a;
+      R.item_c = A.item_c + a;
+      R.item_sep = (G.type == TOS_OBSERVING) ? A.item_sep + a : A.item_sep;
+      R.n_items = b - a;
+      R.next_item = ctr + kChunkCounters + c;
+      const int per_sm = std::max(1, std::min(limit, share->ctas_per_sm(limit)));
+      const cudaError_t ke = launch(R, per_sm);
+      if (ke != cudaSuccess)
+        return fail(TOS_ERR_CUDA, std::string(diag ? "diagonal" : "grid") + " kernel: " + cudaGetErrorString(ke));
+      TOS_CUDA_TRY(cudaEventRecord(done[c % 2], st));
+    }
+    return TOS_OK;
+  };
   if (n_items > 0) {
     TOS_CUDA_TRY(cudaEventRecord(e->ev[2], st));
-    if (use_diag) {
-      PairArgs R = A;
-      R.next_item = ctr + 11;
-      const cudaError_t de = launch_diag_kernel(R, minpos, e->num_sms, st);
-      if (de != cudaSuccess)
-        return fail(TOS_ERR_CUDA, std::string("diagonal kernel: ") + cudaGetErrorString(de));
-    }
+    if (use_diag) TOS_TRY(sweep(true, ctr + 11));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[7], st));
-    if (use_grid) {
-      PairArgs R = A;
-      R.next_item = ctr + 10;
-      const cudaError_t ge2 = launch_grid_kernel(R, G.type, minpos, e->num_sms, st);
-      if (ge2 != cudaSuccess)
-        return fail(TOS_ERR_CUDA, std::string("grid kernel: ") + cudaGetErrorString(ge2));
-    }
+    if (use_grid) TOS_TRY(sweep(false, ctr + 10));
     TOS_CUDA_TRY(cudaEventRecord(e->ev[6], st));
     if (use_runs) {
       PairArgs R = A;

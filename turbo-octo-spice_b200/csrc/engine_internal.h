@@ -104,6 +104,9 @@ struct tos_engine {
   // (kernel variant, warps per CTA)
   std::mutex tune_mu;
   std::map<int, std::pair<int, int>> brute_tuned;
+  // CTAs per SM of the dominant pair-count kernel picked by TOS_XI_TUNE, by
+  // (coordinate type, total bins)
+  std::map<std::pair<int, int>, int> xi_tuned;
 };
 
 struct tos_catalog {
@@ -184,9 +187,21 @@ struct RowPlan {
 // honours TOS_XI_SUBSAMPLES / TOS_XI_PER_GROUP), otherwise into the plan's
 // slots, combined by plan->combine.  Takes the engine lock; the catalogue is
 // only read, so runs with different workspaces may share it.
+// How a run shares the GPU with runs on other streams (the request
+// server): the dominant kernel (grid or diagonal sweep) is launched in
+// chunks of sightline pairs, each as a persistent launch of
+// ctas_per_sm(limit) CTAs per SM (limit: the kernel's occupancy limit),
+// asked again before every chunk, with at most two chunks in flight.  So
+// concurrent requests split the SMs between them, and a request takes over
+// the SMs of one that finished at its next chunk.
+struct SweepShare {
+  std::function<int(int limit)> ctas_per_sm;
+  int chunks = 16;  // chunks per run (fewer when a run has few sightline pairs)
+};
+
 tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos_grid* grid,
                        double scale, uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
-                       tos_xibin* out_cells, tos_xi_stats* stats);
+                       tos_xibin* out_cells, tos_xi_stats* stats, const SweepShare* share = nullptr);
 
 // out[b] = rows[0][b] + rows[1][b] + ... (n_rows x nb XiBins, ascending row order).
 void launch_sum_rows(const tos_xibin* rows, uint32_t n_rows, uint32_t nb, tos_xibin* out,

@@ -14,6 +14,7 @@
 // depend on the order in which pairs are added.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cmath>
@@ -79,7 +80,7 @@ uint64_t workspace_estimate(const tos_catalog* cat, const tos_grid& g, double sc
   bytes += pairs * 20.0;                                      // items (i, j, cos, theta index)
   bytes += n * 24.0;                                          // per primary counts and offsets
   bytes += nc * (near_cells + 12.0) * 4.0;                    // cell neighbours
-  bytes += 4200.0 * 8 + 2.0 * 65536 * (g.axis[0].nbins + 1.0) + 1e6;  // counters, tables, cub
+  bytes += 4192.0 * 8 + 2.0 * 65536 * (g.axis[0].nbins + 1.0) + 1e6;  // counters, tables, cub
   return (uint64_t)bytes;
 }
 
@@ -104,6 +105,9 @@ struct tos_server {
   std::unordered_map<const tos_catalog*, uint64_t> pending;   // unfinished requests per catalogue
   int policy = tos::kFifo;
   double max_wait_s = 5.0;
+  // requests in a slot: each running request's sweep takes its share of the
+  // SMs, ceil(limit / running) CTAs per SM, asked again at every chunk
+  std::atomic<int> running{0};
   uint64_t next_id = 1, completed = 0, peak = 0;
   bool stop = false;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -166,9 +170,19 @@ struct tos_server {
       const size_t nb = (size_t)r->grid.axis[0].nbins * r->grid.axis[1].nbins * r->grid.axis[2].nbins;
       r->bins.assign(nb, tos_xibin{});
       r->rows.assign(r->n_rows * nb, tos_xibin{});
+      tos::SweepShare share;
+      share.ctas_per_sm = [this](int limit) {
+        const int n = std::max(1, running.load());
+        return (limit + n - 1) / n;
+      };
+      // chunks of at least ~128k sightline pairs: a chunk boundary costs the
+      // tail of one launch
+      share.chunks = 16;
+      running.fetch_add(1);
       const tos_status s = tos::xi_run_impl(engines[k], r->cat, ws[k].get(), &r->grid, r->scale,
                                             r->flags, nullptr, r->bins.data(),
-                                            r->n_rows ? r->rows.data() : nullptr, &r->stats);
+                                            r->n_rows ? r->rows.data() : nullptr, &r->stats, &share);
+      running.fetch_sub(1);
       std::string err = (s == TOS_OK) ? std::string() : std::string(tos_last_error());
       const uint64_t held = ws[k]->bytes();
       std::lock_guard<std::mutex> lk(mu);

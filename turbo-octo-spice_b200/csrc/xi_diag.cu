@@ -300,20 +300,30 @@ __global__ void __launch_bounds__(kDiagWarps * 32, 3) diag_kernel(const __grid_c
   add_counters_diag(A, lane, stats[0], stats[1], n_taken);
 }
 
+// Persistent launch: `ctas_per_sm` CTAs per SM (0 or above the occupancy
+// limit: as many as fit), or with `max_out` set only that limit.
 template <bool MINPOS>
-cudaError_t launch_diag(const PairArgs& a, int num_sms, cudaStream_t stream) {
+cudaError_t launch_diag(const PairArgs& a, int num_sms, int ctas_per_sm, cudaStream_t stream, int* max_out) {
   int per_sm = 0;
   const cudaError_t e =
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_kernel<MINPOS>, kDiagWarps * 32, 0);
   if (e != cudaSuccess) return e;
-  diag_kernel<MINPOS><<<num_sms * (per_sm > 0 ? per_sm : 1), kDiagWarps * 32, 0, stream>>>(a);
+  per_sm = per_sm > 0 ? per_sm : 1;
+  if (max_out) {
+    *max_out = per_sm;
+    return cudaSuccess;
+  }
+  if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
+  diag_kernel<MINPOS><<<num_sms * per_sm, kDiagWarps * 32, 0, stream>>>(a);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_diag_kernel(const PairArgs& a, bool minpos, int num_sms, cudaStream_t stream) {
-  return minpos ? launch_diag<true>(a, num_sms, stream) : launch_diag<false>(a, num_sms, stream);
+cudaError_t launch_diag_kernel(const PairArgs& a, bool minpos, int num_sms, int ctas_per_sm, cudaStream_t stream,
+                               int* max_out) {
+  return minpos ? launch_diag<true>(a, num_sms, ctas_per_sm, stream, max_out)
+                : launch_diag<false>(a, num_sms, ctas_per_sm, stream, max_out);
 }
 
 }  // namespace tos

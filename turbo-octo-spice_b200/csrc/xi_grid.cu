@@ -14,6 +14,8 @@
 // consecutive runs [B[t], B[t+1]), t = 0 .. 2 n0, each of one first-axis bin
 // (run n0 is the |x1 - x2| < T[0] gap), so neighbouring lanes share a
 // boundary: a lane reads one table entry per row and evaluates one column.
+#include <algorithm>
+
 #include "xi_sweep.cuh"
 
 namespace tos {
@@ -233,24 +235,33 @@ __global__ void __launch_bounds__(kGridThreads, 4) grid_kernel(const __grid_cons
 }
 
 // Persistent launch: as many CTAs as fit on the SMs at once.
+// Persistent launch: `ctas_per_sm` CTAs per SM (0 or above the occupancy
+// limit: as many as fit), or with `max_out` set only that limit.
 template <int COORD, bool MINPOS>
-cudaError_t launch_grid(const PairArgs& a, int num_sms, cudaStream_t stream) {
+cudaError_t launch_grid(const PairArgs& a, int num_sms, int ctas_per_sm, cudaStream_t stream, int* max_out) {
   int per_sm = 0;
   const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm, grid_kernel<COORD, MINPOS>, kGridThreads, 0);
   if (e != cudaSuccess) return e;
-  grid_kernel<COORD, MINPOS><<<num_sms * (per_sm > 0 ? per_sm : 1), kGridThreads, 0, stream>>>(a);
+  per_sm = std::max(per_sm, 1);
+  if (max_out) {
+    *max_out = per_sm;
+    return cudaSuccess;
+  }
+  if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
+  grid_kernel<COORD, MINPOS><<<num_sms * per_sm, kGridThreads, 0, stream>>>(a);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_grid_kernel(const PairArgs& a, int coord, bool minpos, int num_sms,
-                               cudaStream_t stream) {
+cudaError_t launch_grid_kernel(const PairArgs& a, int coord, bool minpos, int num_sms, int ctas_per_sm,
+                               cudaStream_t stream, int* max_out) {
   if (coord == TOS_CARTESIAN)
-    return minpos ? launch_grid<kCart, true>(a, num_sms, stream)
-                  : launch_grid<kCart, false>(a, num_sms, stream);
-  return minpos ? launch_grid<kObs, true>(a, num_sms, stream) : launch_grid<kObs, false>(a, num_sms, stream);
+    return minpos ? launch_grid<kCart, true>(a, num_sms, ctas_per_sm, stream, max_out)
+                  : launch_grid<kCart, false>(a, num_sms, ctas_per_sm, stream, max_out);
+  return minpos ? launch_grid<kObs, true>(a, num_sms, ctas_per_sm, stream, max_out)
+                : launch_grid<kObs, false>(a, num_sms, ctas_per_sm, stream, max_out);
 }
 
 }  // namespace tos

@@ -140,12 +140,15 @@ size_t pair_kernel_smem(int win_slots);
 
 // Launch the persistent grid-sweep kernel (xi_grid.cu) over the items that
 // run_item() accepts and whose two sightlines lie on the common grid.
-cudaError_t launch_grid_kernel(const PairArgs& a, int coord, bool minpos, int num_sms,
-                               cudaStream_t stream);
+// ctas_per_sm: CTAs per SM (0: as many as fit); with max_out set, only
+// report that limit.
+cudaError_t launch_grid_kernel(const PairArgs& a, int coord, bool minpos, int num_sms, int ctas_per_sm,
+                               cudaStream_t stream, int* max_out = nullptr);
 
 // Launch the persistent diagonal-sweep kernel (xi_diag.cu) over the Polar
 // items that diag_item() accepts (every field on the wide scale).
-cudaError_t launch_diag_kernel(const PairArgs& a, bool minpos, int num_sms, cudaStream_t stream);
+cudaError_t launch_diag_kernel(const PairArgs& a, bool minpos, int num_sms, int ctas_per_sm, cudaStream_t stream,
+                               int* max_out = nullptr);
 
 // Launch the persistent run-sweep kernel (xi_runs.cu) over the items that
 // run_item() accepts: Cartesian and observing coordinates, catalogue sorted

@@ -24,6 +24,7 @@ POLAR, CARTESIAN, OBSERVING = 0, 1, 2
 XI_SUBSAMPLES = 0x1
 XI_EXACT = 0x2
 XI_PER_GROUP = 0x4
+XI_TUNE = 0x8
 
 # numpy views of the C structs
 PIXEL_DTYPE = np.dtype([("value", "<f4"), ("loglam", "<f4"), ("weight", "<f4"), ("distance", "<f4")])
@@ -303,11 +304,13 @@ class Catalog:
 
 
 def xi_run(engine: Engine, catalog: Catalog, grid: Grid, scale: float, subsamples: bool = False,
-           exact: bool = False, per_group: bool = False):
+           exact: bool = False, per_group: bool = False, tune: bool = False):
     """Pair count of XiEstimator::run. Returns (bins, rows or None, stats dict);
     bins/rows are raw (unfinalized) XiBin sums as XIBIN_DTYPE arrays.  rows
     are per cell with subsamples=True, per sightline group (ascending group
-    id, one xi per batched catalogue) with per_group=True."""
+    id, one xi per batched catalogue) with per_group=True.  tune=True first
+    times the dominant kernel's launch shapes on a sample of the sightline
+    pairs and keeps the fastest on the engine (TOS_XI_TUNE)."""
     nb = grid.nbins
     bins = np.zeros(nb, dtype=XIBIN_DTYPE)
     cells = None
@@ -316,7 +319,7 @@ def xi_run(engine: Engine, catalog: Catalog, grid: Grid, scale: float, subsample
     elif per_group:
         cells = np.zeros((catalog.num_groups(), nb), dtype=XIBIN_DTYPE)
     flags = ((XI_SUBSAMPLES if subsamples else 0) | (XI_EXACT if exact else 0) |
-             (XI_PER_GROUP if per_group else 0))
+             (XI_PER_GROUP if per_group else 0) | (XI_TUNE if tune else 0))
     st = XiStats()
     _check(lib().tos_xi_run(engine.handle, catalog.handle, C.byref(grid.c_struct()), scale, flags, _ptr(bins),
                             _ptr(cells) if cells is not None else None, C.byref(st)))

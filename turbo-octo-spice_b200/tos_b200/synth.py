@@ -292,6 +292,26 @@ def mock_batch(n_mocks: int = 256, seed: int = 11, n_range=(2000, 40000), densit
     return parts, scale
 
 
+def mock_batch_stratified(n_pick: int = 32, n_mocks: int = 256, seed: int = 11, n_range=(2000, 40000),
+                          density: float = 16.0, **kw):
+    """A size-stratified sample of the seeded n_mocks-mock draw: the mocks at
+    ranks 0, s, 2s, ... of the draw sorted by sightline count (s = n_mocks /
+    n_pick), so the sample holds the smallest mock and spans the range.  Each
+    mock is generated exactly as in mock_batch (its own seed and cap).
+    Returns (parts, scale, indices) with the mocks' indices in the draw."""
+    counts = mock_counts(n_mocks, seed, n_range)
+    order = np.argsort(counts, kind="stable")
+    step = max(1, n_mocks // n_pick)
+    idx = np.sort(order[::step][:n_pick])
+    parts, scale = [], None
+    for k in idx:
+        n = int(counts[k])
+        los, px, meta = cap_patch(n, seed * 1000 + int(k), float(n) / density, **kw)
+        parts.append((los, px))
+        scale = meta["scale"] if scale is None else min(scale, meta["scale"])
+    return parts, scale, idx
+
+
 def grf_grid(n: int = 64, box: float = 256.0, seed: int = 3, index: float = -2.0) -> np.ndarray:
     """Gaussian random field with P(k) ~ k^index on an n^3 periodic box, unit
     variance, as (n^3, 5) float32 rows x, y, z, delta, w at cell centres."""
