@@ -1,13 +1,15 @@
 """The request server (tos_server): continuous admission of xi requests to
-worker slots under a device-memory budget.
+worker slots under a device-memory budget, and chunk-level scheduling of
+their sweeps.
 
 Pass criteria: every request's result is bit-identical to tos_xi_run on the
 same catalogue alone (bins, per-group rows, pair counts), whatever else runs
 beside it; requests on different slots overlap in time; under a budget that
 holds one workspace at a time they run one after another and still give the
 same results; FIFO starts requests in arrival order, shortest-first may
-reorder them but gives the same results; requests and catalogues that
-cannot fit are refused."""
+reorder them but gives the same results, and a short request that arrives
+while a long one sweeps finishes first; requests and catalogues that cannot
+fit are refused."""
 import numpy as np
 import pytest
 
@@ -177,3 +179,33 @@ def test_subsample_rows_through_the_server(engine, catalogs):
     assert_identical(bins, rb, "bins")
     for c in range(rows.shape[0]):
         assert_identical(rows[c], rc[c], f"cell {c}")
+
+
+def test_short_request_overtakes_long_sweep(engine, catalogs):
+    """A long request's sweep runs as a chain of chunks; with the
+    shortest-first order a short request submitted while it sweeps takes the
+    GPU at the long one's next chunk and finishes first.  Both results equal
+    their lone runs."""
+    import time
+    los, px, meta = T.synth.full_survey(20000, seed=7, area_deg2=1250.0)
+    big = T.Catalog(engine, los, px, 6)
+    small, s_scale = catalogs["a"]
+    g = GRIDS["cartesian"]
+    ref_big = T.xi_run(engine, big, g, meta["scale"])[0]
+    ref_small = T.xi_run(engine, small, g, s_scale)[0]
+    try:
+        with T.Server(0, slots=2, memory_budget_bytes=40 * 10**9) as srv:
+            srv.set_policy("shortest", max_wait_s=30.0)
+            srv.attach(big)
+            srv.attach(small)
+            rb = srv.submit(big, g, meta["scale"])
+            time.sleep(0.05)
+            rs = srv.submit(small, g, s_scale)
+            bb, _, st_b, ib = rb.wait()
+            bs, _, _, i_s = rs.wait()
+    finally:
+        big.close()
+    assert st_b["num_sightline_pairs_used"] > 2 * 131072  # several chunks
+    assert_identical(bb, ref_big, "long request")
+    assert_identical(bs, ref_small, "short request")
+    assert i_s["start_s"] < ib["end_s"] and i_s["end_s"] < ib["end_s"]

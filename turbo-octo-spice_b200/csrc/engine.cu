@@ -932,6 +932,9 @@ constexpr int kMaxChunks = 64;
 constexpr uint64_t kChunkItemsMin = 131072;  // tens of ms per chunk: the launch tail stays small
 constexpr size_t kCounterWords = kChunkCounters + kMaxChunks;
 
+// Host callback after a shared-GPU sweep chunk: hands the SMs back.
+static void CUDART_CB sweep_chunk_done(void* share) { static_cast<SweepShare*>(share)->release(); }
+
 // Fixed-point scales for kernels whose FP64 register sums can hold a whole
 // item's pairs of a bin (at most max_np^2 pairs): every field takes the wide
 // 62-bit conversion (the run, grid and diagonal sweeps).
@@ -1371,29 +1374,12 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
         return fail(TOS_ERR_CUDA, std::string(diag ? "diagonal" : "grid") + " kernel: " + cudaGetErrorString(ke));
       return TOS_OK;
     }
-    int limit = 1;
-    {
-      PairArgs R = A;
-      const cudaError_t qe = diag ? launch_diag_kernel(R, minpos, e->num_sms, 0, st, &limit)
-                                  : launch_grid_kernel(R, G.type, minpos, e->num_sms, 0, st, &limit);
-      if (qe != cudaSuccess) return fail(TOS_ERR_CUDA, std::string("sweep shape: ") + cudaGetErrorString(qe));
-    }
     const uint64_t chunks = std::max<uint64_t>(
         1, std::min<uint64_t>((uint64_t)std::min(std::max(1, share->chunks), kMaxChunks), n_items / kChunkItemsMin));
     const uint64_t per = (n_items + chunks - 1) / chunks;
-    cudaEvent_t done[2] = {nullptr, nullptr};
-    for (auto& ev : done) TOS_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    struct Free {
-      cudaEvent_t* ev;
-      ~Free() {
-        for (int k = 0; k < 2; ++k)
-          if (ev[k]) cudaEventDestroy(ev[k]);
-      }
-    } free_events{done};
     for (uint64_t c = 0; c < chunks; ++c) {
       const uint64_t a = c * per, b = std::min<uint64_t>(n_items, a + per);
       if (a >= b) break;
-      if (c >= 2) TOS_CUDA_TRY(cudaEventSynchronize(done[c % 2]));  // at most two chunks in flight
       PairArgs R = A;
       R.item_i = A.item_i + a;
       R.item_j = A.item_j + a;
@@ -1401,11 +1387,19 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
       R.item_sep = (G.type == TOS_OBSERVING) ? A.item_sep + a : A.item_sep;
       R.n_items = b - a;
       R.next_item = ctr + kChunkCounters + c;
-      const int per_sm = std::max(1, std::min(limit, share->ctas_per_sm(limit)));
+      const uint64_t remaining = (uint64_t)((double)n_pixel_pairs * (double)(n_items - a) / (double)n_items);
+      const int per_sm = share->acquire(remaining);
       const cudaError_t ke = launch(R, per_sm);
-      if (ke != cudaSuccess)
+      if (ke != cudaSuccess) {
+        share->release();
         return fail(TOS_ERR_CUDA, std::string(diag ? "diagonal" : "grid") + " kernel: " + cudaGetErrorString(ke));
-      TOS_CUDA_TRY(cudaEventRecord(done[c % 2], st));
+      }
+      const cudaError_t he = cudaLaunchHostFunc(st, sweep_chunk_done, const_cast<SweepShare*>(share));
+      if (he != cudaSuccess) {
+        cudaStreamSynchronize(st);
+        share->release();
+        return fail(TOS_ERR_CUDA, std::string("chunk callback: ") + cudaGetErrorString(he));
+      }
     }
     return TOS_OK;
   };

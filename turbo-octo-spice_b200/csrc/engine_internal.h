@@ -189,13 +189,16 @@ struct RowPlan {
 // only read, so runs with different workspaces may share it.
 // How a run shares the GPU with runs on other streams (the request
 // server): the dominant kernel (grid or diagonal sweep) is launched in
-// chunks of sightline pairs, each as a persistent launch of
-// ctas_per_sm(limit) CTAs per SM (limit: the kernel's occupancy limit),
-// asked again before every chunk, with at most two chunks in flight.  So
-// concurrent requests split the SMs between them, and a request takes over
-// the SMs of one that finished at its next chunk.
+// chunks of sightline pairs.  Before each chunk the run calls acquire with
+// its remaining pixel pairs (this chunk's included); acquire blocks until the
+// chunk may launch and returns its CTAs per SM (0: as many as fit).  When a
+// chunk's kernel has completed, release is called from a host callback on the
+// run's stream (it must not call CUDA).  The server's scheduler so decides,
+// chunk by chunk, which running request uses the SMs next, while other
+// requests' expansion and result phases run beside it.
 struct SweepShare {
-  std::function<int(int limit)> ctas_per_sm;
+  std::function<int(uint64_t remaining_pairs)> acquire;
+  std::function<void()> release;
   int chunks = 16;  // chunks per run (fewer when a run has few sightline pairs)
 };
 

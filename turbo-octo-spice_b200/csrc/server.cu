@@ -1,20 +1,26 @@
 // server.cu — a request server over resident catalogues: continuous
-// admission of xi requests to worker slots under a device-memory budget.
+// admission of xi requests to worker slots under a device-memory budget, and
+// chunk-level scheduling of their sweeps on the GPU.
 //
 // Each slot owns an engine (its own stream) and a workspace, and runs one
-// request at a time on a host thread of its own, so the requests of
-// different slots overlap on the device: one slot's kernels run while
-// another is in its host phase (neighbour counts, item offsets) or while
-// its own kernels leave SMs idle.  A request is admitted to a free slot as
-// soon as one frees up and its workspace fits in the budget beside the
-// resident catalogues and the other slots' workspaces (admission.h), in
-// arrival order.  Runs on one catalogue never write to it, so any number of
-// slots may count pairs of the same catalogue at once.  The results are
-// those of tos_xi_run on the same catalogue: the fixed-point sums do not
-// depend on the order in which pairs are added.
+// request at a time on a host thread of its own.  A request is admitted to a
+// free slot as soon as one frees up and its workspace fits in the budget
+// beside the resident catalogues and the other slots' workspaces
+// (admission.h), in the server's order (FIFO, or least estimated work
+// first).  Its pair count's dominant kernel runs as a chain of chunks of
+// sightline pairs; the server lets at most two chunks be on the GPU at once
+// and hands the next chunk to the waiting request that comes first in the
+// same order (the shortest-first order uses the remaining work), so the
+// requests of different slots overlap on the device: one request's chunks
+// run while others expand their sightline pairs or read back results, a
+// short request that arrives mid-flight overtakes a long one at its next
+// chunk, and the SMs never idle between chunks.  Runs on one catalogue never
+// write to it, so any number of slots may count pairs of the same catalogue
+// at once.  The results are those of tos_xi_run on the same catalogue: the
+// fixed-point sums do not depend on the order in which pairs are added.
 #include <cuda_runtime.h>
 
-#include <atomic>
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cmath>
@@ -105,9 +111,58 @@ struct tos_server {
   std::unordered_map<const tos_catalog*, uint64_t> pending;   // unfinished requests per catalogue
   int policy = tos::kFifo;
   double max_wait_s = 5.0;
-  // requests in a slot: each running request's sweep takes its share of the
-  // SMs, ceil(limit / running) CTAs per SM, asked again at every chunk
-  std::atomic<int> running{0};
+  // Sweep scheduler: running requests launch their sweep in chunks, at most
+  // kChunksInFlight chunks on the GPU at once (the next one queued behind the
+  // running one, so the SMs never idle between chunks); a chunk that may
+  // launch goes to the waiting request first in the admission order (FIFO:
+  // the oldest; shortest-first: the least remaining work, unless a request
+  // has waited max_wait_s since it was submitted).  A short request that
+  // arrives while a long one sweeps thus takes the SMs at the long one's next
+  // chunk, and every request's expansion and result phases run beside other
+  // requests' chunks.
+  static constexpr int kChunksInFlight = 2;
+  struct ChunkWaiter {
+    uint64_t remaining;
+    double t_submit;
+    uint64_t id;
+  };
+  std::mutex sched_mu;
+  std::condition_variable sched_cv;
+  std::vector<ChunkWaiter*> chunk_waiters;
+  int chunks_in_flight = 0;
+
+  // Whether w goes before v (sched_mu held).
+  bool chunk_before(const ChunkWaiter* w, const ChunkWaiter* v, double t) const {
+    if (policy == tos::kShortest) {
+      const bool ow = t - w->t_submit > max_wait_s, ov = t - v->t_submit > max_wait_s;
+      if (ow != ov) return ow;
+      if (!ow && w->remaining != v->remaining) return w->remaining < v->remaining;
+    }
+    return w->t_submit != v->t_submit ? w->t_submit < v->t_submit : w->id < v->id;
+  }
+
+  int acquire_chunk(tos::Request* r, uint64_t remaining) {
+    std::unique_lock<std::mutex> lk(sched_mu);
+    ChunkWaiter me{remaining, r->t_submit, r->id};
+    chunk_waiters.push_back(&me);
+    sched_cv.wait(lk, [&] {
+      if (chunks_in_flight >= kChunksInFlight) return false;
+      const double t = now();
+      for (const ChunkWaiter* w : chunk_waiters)
+        if (w != &me && chunk_before(w, &me, t)) return false;
+      return true;
+    });
+    chunk_waiters.erase(std::find(chunk_waiters.begin(), chunk_waiters.end(), &me));
+    ++chunks_in_flight;
+    sched_cv.notify_all();
+    return 0;  // the whole GPU: as many CTAs per SM as fit
+  }
+
+  void release_chunk() {
+    std::lock_guard<std::mutex> lk(sched_mu);
+    --chunks_in_flight;
+    sched_cv.notify_all();
+  }
   uint64_t next_id = 1, completed = 0, peak = 0;
   bool stop = false;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -171,18 +226,13 @@ struct tos_server {
       r->bins.assign(nb, tos_xibin{});
       r->rows.assign(r->n_rows * nb, tos_xibin{});
       tos::SweepShare share;
-      share.ctas_per_sm = [this](int limit) {
-        const int n = std::max(1, running.load());
-        return (limit + n - 1) / n;
-      };
-      // chunks of at least ~128k sightline pairs: a chunk boundary costs the
-      // tail of one launch
+      share.acquire = [this, r](uint64_t remaining) { return acquire_chunk(r, remaining); };
+      share.release = [this] { release_chunk(); };
       share.chunks = 16;
-      running.fetch_add(1);
       const tos_status s = tos::xi_run_impl(engines[k], r->cat, ws[k].get(), &r->grid, r->scale,
                                             r->flags, nullptr, r->bins.data(),
                                             r->n_rows ? r->rows.data() : nullptr, &r->stats, &share);
-      running.fetch_sub(1);
+      cudaStreamSynchronize(engines[k]->stream);  // chunk callbacks done before `share` goes
       std::string err = (s == TOS_OK) ? std::string() : std::string(tos_last_error());
       const uint64_t held = ws[k]->bytes();
       std::lock_guard<std::mutex> lk(mu);
