@@ -153,9 +153,6 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
   __syncwarp();
   const unsigned lt = (1u << lane) - 1u;
   const int span = 32 * K;
-  // binning constants in registers
-  const float invf = A.invf, offf = A.offf, mag = A.mag, nbf = A.nbf, nbp1f = A.nbp1f;
-  const int bits = A.bits, kbits = A.k, kmask = (1 << A.k) - 1, nbins = A.nbins, n_last = A.n - 1;
   const long long ngroups = ((long long)A.n - 1 + span - 1) / span;
   unsigned long long n_recheck = 0;
   for (;;) {
@@ -189,17 +186,17 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
       }
     }
     int qn = 0;  // queued runs (the same in every lane)
-    // the lane's newest column, t + d0 + K - 1, clamped to the last point (a
-    // clamped column only ever pairs with `in` false)
-    const int jn = d0 + K - 1;
-    const int j_end = A.n - jn;  // rows t < j_end have the newest column
+    // the lane's newest column (t + d0 + K - 1) and the row, walked by pointer
+    const float4* pj = A.pos + (d0 + K - 1);
+    const double* wdj = A.wd + (d0 + K - 1);
+    const double* wj = A.w + (d0 + K - 1);
+    const int j_end = A.n - (d0 + K - 1);  // rows t < j_end have the newest column
 #pragma unroll 1
     for (int t = 0; t < t_end; ++t) {
-      {
-        const int jc = min(t + jn, n_last);
-        cp[K - 1] = A.pos[jc];
-        cwd[K - 1] = A.wd[jc];
-        cw[K - 1] = A.w[jc];
+      if (t < j_end) {
+        cp[K - 1] = pj[t];
+        cwd[K - 1] = wdj[t];
+        cw[K - 1] = wj[t];
       }
       const float4 pi = A.pos[t];
       const double wdi = A.wd[t], wi = A.w[t];
@@ -209,12 +206,12 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
         const float dx = __fsub_rn(pi.x, cp[m].x), dy = __fsub_rn(pi.y, cp[m].y),
                     dz = __fsub_rn(pi.z, cp[m].z);
         const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
-        const float tt = __fmaf_rn(sqrt_approx(r2), invf, offf);
-        const int qq = __float_as_int(__fadd_rz(tt, mag)) - bits;
-        int b = (qq >> kbits) + 1;
-        b = (tt < 0.f) ? 0 : ((tt >= nbf) ? nbins + 1 : b);
+        const float tt = __fmaf_rn(sqrt_approx(r2), A.invf, A.offf);
+        const int qq = __float_as_int(__fadd_rz(tt, A.mag)) - A.bits;
+        int b = (qq >> A.k) + 1;
+        b = (tt < 0.f) ? 0 : ((tt >= A.nbf) ? A.nbins + 1 : b);
         uint32_t key = in ? (uint32_t)b : 0xFFFFFFFFu;
-        const bool recheck = in && (((qq + 1) & kmask) < 2) && (tt < nbp1f) && (tt > -1.f);
+        const bool recheck = in && (((qq + 1) & ((1 << A.k) - 1)) < 2) && (tt < A.nbp1f) && (tt > -1.f);
         if (__any_sync(kFull, recheck)) {
           if (recheck) {
             key = exact_index(A, pi, cp[m], b);
