@@ -553,6 +553,7 @@ def polar_measure(eng, cat, W, args):
            "sightline_pairs": int(st["num_sightline_pairs_used"])}
     peak = NSM * FP32_LANES_PER_SM * 1965.0 * 1e6
     out["roofline_frac"] = pairs * OPS_PER_PAIR["polar"] / (st["ms_diag"] / 1e3) / peak
+    out["traffic"] = load_traffic(W["name"] + "_polar")
     if not args.no_parity:
         Wp = dict(W, grid=g)
         out["parity"] = parity_measure(eng, cat, Wp, bins)

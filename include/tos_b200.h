@@ -152,6 +152,20 @@ void tos_engine_destroy(tos_engine* engine);
 tos_status tos_catalog_create(tos_engine* engine, const tos_sightline* los, size_t n_los,
                               const tos_pixel* pixels, size_t n_pixels, int healpix_order,
                               tos_catalog** out);
+
+/* tos_catalog_create with every pixel's comoving distance computed on the
+ * device from its loglam for a flat universe of matter density omega_matter
+ * (the pixels' own distance fields are ignored): the redshift and distance of
+ * h5healxi.cc:38-40, 196-203, with the same bits as tos_fill_distances on the
+ * host.  TOS_ERR_INVALID_ARG for a loglam that is not finite or below
+ * log10(1216). */
+tos_status tos_catalog_create_dc(tos_engine* engine, const tos_sightline* los, size_t n_los,
+                                 const tos_pixel* pixels, size_t n_pixels, int order, double omega_matter,
+                                 tos_catalog** out);
+
+/* The catalogue's per-pixel comoving distances (float, in the compact order
+ * of the catalogue: the pixels of sightline 0, then of sightline 1, ...). */
+tos_status tos_catalog_distances(const tos_catalog* catalog, float* out, size_t capacity);
 void tos_catalog_destroy(tos_catalog* catalog);
 
 /* Number of occupied sky cells (SkyBins::getNBins, SkyBins.h:53). */

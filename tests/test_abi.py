@@ -69,3 +69,14 @@ def test_comoving_distance_matches_fp64_quadrature():
     np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-9)
     # D_C(1.9605) ~ 3586 Mpc/h (the angular scale of the configurations)
     assert abs(T.comoving_distance(0.3, [1.9605])[0] - 3586.0) < 2.0
+
+
+def test_fill_distances_matches_fp64_integral():
+    """tos_fill_distances (host): z from loglam (h5healxi.cc:38-40) and D_C from
+    the table, against an FP64 quadrature of the same integral, to within one
+    float rounding."""
+    los, px, meta = synth.small_patch(200, seed=3)
+    got = T.fill_distances(0.3, px)["distance"].astype(np.float64)
+    z = 10.0 ** (px["loglam"].astype(np.float64) - np.log10(1216.0)) - 1.0
+    ref = synth.comoving_distance_fp64(z, 0.3)
+    assert np.max(np.abs(got - ref) / ref) < 1.2e-7

@@ -1,4 +1,6 @@
-// cosmology.cc — flat LCDM line-of-sight comoving distance in Mpc/h.
+// cosmology.cc — flat LCDM line-of-sight comoving distance in Mpc/h (host
+// side: the table, tos_comoving_distance, tos_fill_distances; the per-pixel
+// arithmetic is cosmology.h's, shared with the device fill).
 //
 // Replaces cosmo::LambdaCdmUniverse::getLineOfSightComovingDistance and the
 // loglam -> distance loop of h5healxi (h5healxi.cc:38-40, 123-131, 196-203):
@@ -8,6 +10,8 @@
 // 16-point Gauss-Legendre panels (error far below 1e-14 relative), and
 // evaluated between nodes by cubic Hermite interpolation using the exact
 // derivative 1/E at the nodes.
+#include "cosmology.h"
+
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -15,8 +19,6 @@
 #include "../../include/tos_b200.h"
 
 namespace {
-
-constexpr double kHubbleDistance = 2997.92458;  // c / (100 km/s/Mpc) in Mpc/h
 
 // 16-point Gauss-Legendre nodes/weights on [-1, 1] (positive half).
 constexpr double kGLx[8] = {0.0950125098376374, 0.2816035507792589, 0.4580167776572274,
@@ -29,18 +31,14 @@ constexpr double kGLw[8] = {0.1894506104550685, 0.1826034150449236, 0.1691565193
 struct Table {
   double om = -1;
   double dz = 1e-3;
-  std::vector<double> d;  // D_C at z = k*dz
+  std::vector<double> d;  // D_C at z = k*dz, in units of c / (100 km/s/Mpc)
 };
-
-inline double inv_e(double om, double z) {
-  const double a = 1.0 + z;
-  return 1.0 / std::sqrt(om * a * a * a + (1.0 - om));
-}
 
 double panel(double om, double z0, double z1) {
   const double h = 0.5 * (z1 - z0), m = 0.5 * (z1 + z0);
   double s = 0;
-  for (int k = 0; k < 8; ++k) s += kGLw[k] * (inv_e(om, m - h * kGLx[k]) + inv_e(om, m + h * kGLx[k]));
+  for (int k = 0; k < 8; ++k)
+    s += kGLw[k] * (tos::inv_e_hd(om, m - h * kGLx[k]) + tos::inv_e_hd(om, m + h * kGLx[k]));
   return s * h;
 }
 
@@ -63,21 +61,20 @@ const Table& table_for(double om, double zmax) {
   return g_table;
 }
 
-inline double eval(const Table& t, double z) {
-  // z in units of the table step
-  const double u = z / t.dz;
-  size_t k = (size_t)u;
-  if (k + 1 >= t.d.size()) k = t.d.size() - 2;
-  const double s = u - (double)k;
-  const double h = t.dz;
-  const double y0 = t.d[k], y1 = t.d[k + 1];
-  const double m0 = inv_e(t.om, k * h) * h, m1 = inv_e(t.om, (k + 1) * h) * h;
-  const double s2 = s * s, s3 = s2 * s;
-  return (2 * s3 - 3 * s2 + 1) * y0 + (s3 - 2 * s2 + s) * m0 + (-2 * s3 + 3 * s2) * y1 +
-         (s3 - s2) * m1;
+}  // namespace
+
+namespace tos {
+
+double log_lya() { return std::log10(1216.0); }  // turbooctospice::logLyA (constants.h:7-8)
+
+void dc_table(double om, double zmax, std::vector<double>* d, double* dz) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  const Table& t = table_for(om, zmax);
+  *d = t.d;
+  *dz = t.dz;
 }
 
-}  // namespace
+}  // namespace tos
 
 extern "C" tos_status tos_comoving_distance(double omega_matter, const double* z, size_t n,
                                             double* out) {
@@ -89,24 +86,23 @@ extern "C" tos_status tos_comoving_distance(double omega_matter, const double* z
   }
   std::lock_guard<std::mutex> lock(g_mu);
   const Table& t = table_for(omega_matter, zmax);
-  for (size_t k = 0; k < n; ++k) out[k] = kHubbleDistance * eval(t, z[k]);
+  for (size_t k = 0; k < n; ++k)
+    out[k] = tos::dmul(tos::kHubbleDistance, tos::dc_eval_hd(t.d.data(), t.d.size(), t.om, t.dz, z[k]));
   return TOS_OK;
 }
 
 extern "C" tos_status tos_fill_distances(double omega_matter, tos_pixel* px, size_t n) {
-  const double kLogLyA = std::log10(1216.0);  // turbooctospice::logLyA (constants.h:7-8)
+  const double lya = tos::log_lya();
   if ((n && !px) || !(omega_matter > 0 && omega_matter <= 1)) return TOS_ERR_INVALID_ARG;
   double zmax = 0;
   for (size_t k = 0; k < n; ++k) {
-    const double z = std::pow(10.0, (double)px[k].loglam - kLogLyA) - 1.0;  // h5healxi.cc:38-40
+    const double z = tos::pixel_z_hd(px[k].loglam, lya);  // h5healxi.cc:38-40
     if (!(z >= 0) || !std::isfinite(z)) return TOS_ERR_INVALID_ARG;
     zmax = std::max(zmax, z);
   }
   std::lock_guard<std::mutex> lock(g_mu);
   const Table& t = table_for(omega_matter, zmax);
-  for (size_t k = 0; k < n; ++k) {
-    const double z = std::pow(10.0, (double)px[k].loglam - kLogLyA) - 1.0;
-    px[k].distance = (float)(kHubbleDistance * eval(t, z));
-  }
+  for (size_t k = 0; k < n; ++k)
+    px[k].distance = tos::pixel_distance_hd(px[k].loglam, lya, t.d.data(), t.d.size(), t.om, t.dz);
   return TOS_OK;
 }

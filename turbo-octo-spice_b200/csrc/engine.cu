@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "cosmology.h"
 #include "engine_internal.h"
 #include "healpix.h"
 #include "fixed128.cuh"
@@ -588,6 +589,80 @@ tos_status ensure_grid(tos_engine* e, tos_catalog* cat, int w, cudaStream_t st) 
   return TOS_OK;
 }
 
+// Smallest and largest loglam of the pixels as ordered float bits
+// (mm[0] = min, mm[1] = max), and whether one is not finite (mm[2]).
+__device__ __forceinline__ unsigned int float_order(float f) {
+  const unsigned int u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void k_loglam_range(const tos_pixel* px, size_t n, unsigned int* mm) {
+  unsigned int lo = 0xFFFFFFFFu, hi = 0u, bad = 0u;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const float l = px[k].loglam;
+    if (!isfinite(l)) bad = 1u;
+    const unsigned int o = float_order(l);
+    lo = min(lo, o);
+    hi = max(hi, o);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+    bad |= __shfl_xor_sync(0xFFFFFFFFu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&mm[0], lo);
+    atomicMax(&mm[1], hi);
+    if (bad) atomicOr(&mm[2], 1u);
+  }
+}
+
+// Every pixel's distance from its loglam (cosmology.h: the same bits as the
+// host's tos_fill_distances).
+__global__ void k_fill_distances(tos_pixel* px, size_t n, double log_lya, const double* table, size_t nt,
+                                 double om, double dz) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    px[k].distance = pixel_distance_hd(px[k].loglam, log_lya, table, nt, om, dz);
+}
+
+// Fill the distances of the catalogue's device pixels (d_raw, n of them)
+// for a flat universe of matter density `om` (stream st).  Fails like
+// tos_fill_distances on a loglam that is not finite or gives z < 0.
+tos_status fill_distances_device(tos_engine* e, tos_pixel* d_px, size_t n, double om, cudaStream_t st) {
+  if (!(om > 0 && om <= 1)) return fail(TOS_ERR_INVALID_ARG, "omega_matter must be in (0, 1]");
+  if (n == 0) return TOS_OK;
+  DevBuf<unsigned int> mm;
+  TOS_TRY(mm.alloc(3));
+  const unsigned int init[3] = {0xFFFFFFFFu, 0u, 0u};
+  TOS_CUDA_TRY(cudaMemcpyAsync(mm.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_loglam_range<<<grid_for(e, n, 256), 256, 0, st>>>(d_px, n, mm.p);
+  TOS_CUDA_TRY(cudaGetLastError());
+  unsigned int h[3];
+  TOS_CUDA_TRY(cudaMemcpyAsync(h, mm.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));
+  auto unorder = [](unsigned int o) {
+    const unsigned int u = (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+  };
+  const double lya = log_lya();
+  const float lmin = unorder(h[0]), lmax = unorder(h[1]);
+  if (h[2] || !(pixel_z_hd(lmin, lya) >= 0))
+    return fail(TOS_ERR_INVALID_ARG, "pixel loglam must be finite and at least log10(1216)");
+  // one table step of margin above the largest z covers rounding
+  std::vector<double> table;
+  double dz = 0;
+  dc_table(om, pixel_z_hd(lmax, lya) + 2e-3, &table, &dz);
+  DevBuf<double> d_table;
+  TOS_TRY(d_table.alloc(table.size()));
+  TOS_CUDA_TRY(cudaMemcpyAsync(d_table.p, table.data(), table.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  k_fill_distances<<<grid_for(e, n, 256), 256, 0, st>>>(d_px, n, lya, d_table.p, table.size(), om, dz);
+  TOS_CUDA_TRY(cudaGetLastError());
+  TOS_CUDA_TRY(cudaStreamSynchronize(st));  // the table buffer is freed on return
+  return TOS_OK;
+}
+
 // ============================================================================
 // C ABI
 // ============================================================================
@@ -638,6 +713,24 @@ void tos_engine_destroy(tos_engine* e) {
 tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_los,
                               const tos_pixel* pixels, size_t n_pixels, int order,
                               tos_catalog** out) {
+  return tos::catalog_create_impl(e, los, n_los, pixels, n_pixels, order, 0.0, out);
+}
+
+tos_status tos_catalog_create_dc(tos_engine* e, const tos_sightline* los, size_t n_los,
+                                 const tos_pixel* pixels, size_t n_pixels, int order, double omega_matter,
+                                 tos_catalog** out) {
+  if (!(omega_matter > 0 && omega_matter <= 1))
+    return fail(TOS_ERR_INVALID_ARG, "omega_matter must be in (0, 1]");
+  return tos::catalog_create_impl(e, los, n_los, pixels, n_pixels, order, omega_matter, out);
+}
+
+}  // extern "C"
+
+// Catalogue creation; omega_matter > 0: each pixel's distance is computed on
+// the device from its loglam (the pixels' own distances are ignored).
+tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, size_t n_los,
+                                    const tos_pixel* pixels, size_t n_pixels, int order, double omega_matter,
+                                    tos_catalog** out) {
   if (!e || !out) return fail(TOS_ERR_INVALID_ARG, "engine/out is null");
   *out = nullptr;
   if (n_los == 0 || !los) return fail(TOS_ERR_INVALID_ARG, "no sightlines");
@@ -796,6 +889,7 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
     TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_flags.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
   }
   TOS_CUDA_TRY(cudaMemsetAsync(cat->d_maxes.p, 0, 4 * sizeof(double), st));
+  if (omega_matter > 0) TOS_TRY(fill_distances_device(e, cat->d_raw.p, total, omega_matter, st));
   k_fill<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_dist_pad.p, padded, kSentinel);
   k_fill<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_loglam_pad.p, padded, kSentinel);
   k_prep<<<grid_for(e, n_los * 32, 256), 256, 0, st>>>(
@@ -831,6 +925,41 @@ tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_
   // the raw copy is no longer needed
   cat->d_raw.release();
   *out = cat.release();
+  return TOS_OK;
+}
+
+namespace tos {
+namespace {
+// Compact copy of the padded per-pixel distances (pixel p of sightline s at
+// off[s] + p).
+__global__ void k_gather_distances(const float* dist_pad, const uint64_t* off, const uint32_t* npix, size_t n_los,
+                                   float* out) {
+  const int lane = threadIdx.x & 31;
+  for (size_t s = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32; s < n_los;
+       s += (size_t)gridDim.x * blockDim.x / 32) {
+    const float* src = dist_pad + off[s] + (uint64_t)kPad * (s + 1);
+    for (uint32_t p = lane; p < npix[s]; p += 32) out[off[s] + p] = src[p];
+  }
+}
+}  // namespace
+}  // namespace tos
+
+extern "C" {
+
+tos_status tos_catalog_distances(const tos_catalog* c, float* out, size_t cap) {
+  if (!c || (!out && c->n_pix)) return fail(TOS_ERR_INVALID_ARG, "null argument");
+  if (cap < c->n_pix) return fail(TOS_ERR_INVALID_ARG, "capacity too small");
+  if (c->n_pix == 0) return TOS_OK;
+  tos_engine* e = c->eng;
+  std::lock_guard<std::mutex> lock(e->mu);
+  DeviceGuard g(e->device);
+  DevBuf<float> tmp;
+  TOS_TRY(tmp.alloc(c->n_pix));
+  k_gather_distances<<<grid_for(e, c->n_los * 32, 256), 256, 0, e->stream>>>(c->d_dist_pad.p, c->d_off.p,
+                                                                           c->d_npix.p, c->n_los, tmp.p);
+  TOS_CUDA_TRY(cudaGetLastError());
+  TOS_CUDA_TRY(cudaMemcpyAsync(out, tmp.p, c->n_pix * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+  TOS_CUDA_TRY(cudaStreamSynchronize(e->stream));
   return TOS_OK;
 }
 

@@ -187,6 +187,12 @@ struct RowPlan {
 // honours TOS_XI_SUBSAMPLES / TOS_XI_PER_GROUP), otherwise into the plan's
 // slots, combined by plan->combine.  Takes the engine lock; the catalogue is
 // only read, so runs with different workspaces may share it.
+// Catalogue creation behind tos_catalog_create and tos_catalog_create_dc;
+// omega_matter > 0: each pixel's distance is computed on the device from its
+// loglam (the pixels' own distances are ignored).
+tos_status catalog_create_impl(tos_engine* e, const tos_sightline* los, size_t n_los, const tos_pixel* pixels,
+                               size_t n_pixels, int order, double omega_matter, tos_catalog** out);
+
 // How a run shares the GPU with runs on other streams (the request
 // server): the dominant kernel (grid or diagonal sweep) is launched in
 // chunks of sightline pairs.  Before each chunk the run calls acquire with

@@ -130,6 +130,8 @@ def lib() -> C.CDLL:
         L.tos_catalog_device_bytes.argtypes = [vp, C.POINTER(u64)]
         L.tos_comoving_distance.argtypes = [dbl, vp, sz, vp]
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
+        L.tos_catalog_create_dc.argtypes = [vp, vp, sz, vp, sz, i32, dbl, C.POINTER(vp)]
+        L.tos_catalog_distances.argtypes = [vp, vp, sz]
         for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
                      "tos_catalog_sightline_cells", "tos_grid_max_angular_scale", "tos_xi_run",
                      "tos_brute_run", "tos_brute_tune", "tos_comoving_distance", "tos_fill_distances"):
@@ -245,15 +247,30 @@ class Engine:
 class Catalog:
     """Sightlines and pixels resident on the device, binned into HEALPix cells."""
 
-    def __init__(self, engine: Engine, sightlines: np.ndarray, pixels: np.ndarray, healpix_order: int):
+    def __init__(self, engine: Engine, sightlines: np.ndarray, pixels: np.ndarray, healpix_order: int,
+                 omega_matter: float = None):
+        """With omega_matter, each pixel's comoving distance is computed on the
+        device from its loglam (tos_catalog_create_dc; the pixels' own
+        distances are ignored), with the same bits as fill_distances."""
         sightlines = np.ascontiguousarray(sightlines, dtype=SIGHTLINE_DTYPE)
         pixels = np.ascontiguousarray(pixels, dtype=PIXEL_DTYPE)
         h = C.c_void_p()
-        _check(lib().tos_catalog_create(engine.handle, _ptr(sightlines), len(sightlines), _ptr(pixels),
-                                        len(pixels), healpix_order, C.byref(h)))
+        if omega_matter is None:
+            _check(lib().tos_catalog_create(engine.handle, _ptr(sightlines), len(sightlines), _ptr(pixels),
+                                            len(pixels), healpix_order, C.byref(h)))
+        else:
+            _check(lib().tos_catalog_create_dc(engine.handle, _ptr(sightlines), len(sightlines), _ptr(pixels),
+                                               len(pixels), healpix_order, float(omega_matter), C.byref(h)))
         self._h = h
         self.engine = engine
         self.n_sightlines = len(sightlines)
+        self.n_pixels = int(sightlines["num_pixels"].astype(np.int64).sum())
+
+    def distances(self) -> np.ndarray:
+        """The resident per-pixel comoving distances (compact sightline order)."""
+        out = np.zeros(self.n_pixels, dtype=np.float32)
+        _check(lib().tos_catalog_distances(self._h, _ptr(out), len(out)))
+        return out
 
     @property
     def handle(self):
@@ -504,6 +521,14 @@ def jackknife(engine: Engine, cat: "Catalog", region_order: int, nbins: int):
     _check(lib().tos_xi_jackknife(engine.handle, cat.handle, region_order, n.value, C.byref(n), _ptr(ids),
                                   _ptr(xi), _ptr(cov)))
     return ids, xi, cov
+
+
+def fill_distances(omega_matter: float, pixels: np.ndarray) -> np.ndarray:
+    """tos_fill_distances on the host: a copy of the pixels with each distance
+    computed from its loglam (h5healxi.cc:38-40, 196-203)."""
+    out = np.ascontiguousarray(pixels, dtype=PIXEL_DTYPE).copy()
+    _check(lib().tos_fill_distances(omega_matter, _ptr(out), len(out)))
+    return out
 
 
 def comoving_distance(omega_matter: float, z) -> np.ndarray:
