@@ -37,6 +37,16 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 
 // ---- catalogue preparation -------------------------------------------------
 
+__global__ void k_fill_pack(PixPack* p, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    PixPack q;
+    q.d = kSentinel;
+    q.w = 0.f;
+    q.wd = 0.0;
+    p[k] = q;
+  }
+}
+
 __global__ void k_fill(float* p, size_t n, float v) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
        k += (size_t)gridDim.x * blockDim.x)
@@ -47,7 +57,7 @@ __global__ void k_fill(float* p, size_t n, float v) {
 // w*delta (exact product of two floats in double), weights; exclusive prefix
 // sums of (w*delta, w, loglam); coordinate ranges; sortedness.
 __global__ void k_prep(const tos_pixel* raw, const uint64_t* off, const uint32_t* npix,
-                       size_t n_los, float* dist_pad, float* loglam_pad, double* wd, float* w,
+                       size_t n_los, float* dist_pad, float* loglam_pad, PixPack* pack, double* wd, float* w,
                        double4* prefix, float4* range, unsigned int* flags,
                        unsigned long long* maxbits) {
   const int lane = threadIdx.x & 31;
@@ -76,6 +86,11 @@ __global__ void k_prep(const tos_pixel* raw, const uint64_t* off, const uint32_t
         v2 = (double)px.loglam;
         wd[o + k] = v0;
         w[o + k] = px.weight;
+        PixPack q;
+        q.d = px.distance;
+        q.w = px.weight;
+        q.wd = v0;
+        pack[po + k] = q;
         dmin = fminf(dmin, px.distance);
         dmax = fmaxf(dmax, px.distance);
         lmin = fminf(lmin, px.loglam);
@@ -847,6 +862,7 @@ tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, siz
   const size_t padded = total + (size_t)kPad * (n_los + 1);
   TOS_TRY(cat->d_dist_pad.alloc(padded));
   TOS_TRY(cat->d_loglam_pad.alloc(padded));
+  TOS_TRY(cat->d_pack.alloc(padded));
   TOS_TRY(cat->d_wd.alloc(total));
   TOS_TRY(cat->d_w.alloc(total));
   TOS_TRY(cat->d_prefix.alloc(total + n_los));
@@ -892,8 +908,9 @@ tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, siz
   if (omega_matter > 0) TOS_TRY(fill_distances_device(e, cat->d_raw.p, total, omega_matter, st));
   k_fill<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_dist_pad.p, padded, kSentinel);
   k_fill<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_loglam_pad.p, padded, kSentinel);
+  k_fill_pack<<<grid_for(e, padded, 256), 256, 0, st>>>(cat->d_pack.p, padded);
   k_prep<<<grid_for(e, n_los * 32, 256), 256, 0, st>>>(
-      cat->d_raw.p, cat->d_off.p, cat->d_npix.p, n_los, cat->d_dist_pad.p, cat->d_loglam_pad.p,
+      cat->d_raw.p, cat->d_off.p, cat->d_npix.p, n_los, cat->d_dist_pad.p, cat->d_loglam_pad.p, cat->d_pack.p,
       cat->d_wd.p, cat->d_w.p, cat->d_prefix.p, cat->d_range.p, cat->d_flags.p,
       (unsigned long long*)cat->d_maxes.p);
   TOS_CUDA_TRY(cudaGetLastError());
@@ -1040,7 +1057,8 @@ uint64_t catalog_data_bytes(const tos_catalog* c) {
   uint64_t b = c->d_trig.bytes() + c->d_cap.bytes() + c->d_cell_grange.bytes() +
                c->d_group_cell_start.bytes() + c->d_cell_idx.bytes() + c->d_cell_start.bytes() +
                c->d_members.bytes() + c->d_npix.bytes() + c->d_off.bytes() + c->d_raw.bytes() +
-               c->d_dist_pad.bytes() + c->d_loglam_pad.bytes() + c->d_wd.bytes() + c->d_w.bytes() +
+               c->d_dist_pad.bytes() + c->d_loglam_pad.bytes() + c->d_pack.bytes() + c->d_wd.bytes() +
+               c->d_w.bytes() +
                c->d_prefix.bytes() + c->d_range.bytes() + c->d_flags.bytes() + c->d_maxes.bytes();
   for (int w = 0; w < 2; ++w) b += c->d_grid[w].bytes() + c->d_gfirst[w].bytes();
   return b;
@@ -1254,6 +1272,7 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
   A.npix = cat->d_npix.p;
   A.dist_pad = cat->d_dist_pad.p;
   A.loglam_pad = cat->d_loglam_pad.p;
+  A.pack = cat->d_pack.p;
   A.wd = cat->d_wd.p;
   A.w = cat->d_w.p;
   A.prefix = cat->d_prefix.p;

@@ -135,6 +135,7 @@ struct tos_catalog {
   tos::DevBuf<uint64_t> d_off;      // compact offset (per-pixel double/float arrays)
   tos::DevBuf<tos_pixel> d_raw;     // uploaded pixels, compact order
   tos::DevBuf<float> d_dist_pad, d_loglam_pad;
+  tos::DevBuf<tos::PixPack> d_pack;  // padded like d_dist_pad
   tos::DevBuf<double> d_wd;         // w*delta per pixel, exact in double
   tos::DevBuf<float> d_w;           // weight per pixel
   tos::DevBuf<double4> d_prefix;    // per sightline N+1 exclusive prefix sums of (w*delta, w, loglam)

@@ -33,6 +33,14 @@ constexpr int kPad = 32;
 // finite so that differences of sentinels never produce NaN.
 constexpr float kSentinel = 1.0e30f;
 
+// A pixel's distance, weight and w*delta in one 16-byte load (the padded
+// layout of the distance array; padding entries have distance kSentinel and
+// zero weights).
+struct alignas(16) PixPack {
+  float d, w;
+  double wd;
+};
+
 // ---- exact scalar ops -------------------------------------------------------
 #ifdef __CUDA_ARCH__
 TOS_HD double dmul(double a, double b) { return __dmul_rn(a, b); }

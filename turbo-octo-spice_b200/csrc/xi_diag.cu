@@ -90,6 +90,8 @@ struct DItem {
   const double* colwd;
   const float* colw;
   const double4* prej;
+  const PixPack* rowp;   // padded (distance, weight, w*delta) of sightline i
+  const PixPack* colp;   // the same of sightline j
 };
 
 // Add the run [s0, s1) of diagonal delta with key `key` to row `cell`
@@ -163,13 +165,16 @@ __device__ __forceinline__ void diag_group(const PairArgs& A, const DItem& it, i
     // distances: p2 >= s_lo + delta0 >= -31 and p2 < s_hi + delta0 + 32 <= nj + 32
     const int p2 = s + delta;
     const bool in = lane_on && (unsigned)p2 < (unsigned)it.nj;
+    // one 16-byte load each: the row's (broadcast) and the lane's column's
+    // distance, weight and w*delta (padding: sentinel distance, zero weights)
+    const PixPack rp = it.rowp[s], cq = it.colp[p2];
     DRow R;
-    R.d1 = it.rowd[s];
+    R.d1 = rp.d;
     R.x1 = R.d1;
     const float p = __fmul_rn(R.d1, R.d1);
     R.dl1 = -__fmaf_rn(R.d1, R.d1, -p);  // -(d1*d1 - fl(d1*d1)), exact
     R.A1 = __fmul_rn(R.d1, it.ap);
-    const float x2 = it.cold[p2];
+    const float x2 = cq.d;
     bool recheck;
     uint32_t key = polar_key<MINPOS>(A, R, x2, recheck);
     recheck = recheck && in;
@@ -200,8 +205,8 @@ __device__ __forceinline__ void diag_group(const PairArgs& A, const DItem& it, i
       wgt = 0.0;
     }
     if (key != kInvalidKey) {  // binned: p2 is a pixel of sightline j
-      didj = __fma_rn(it.rowwd[s], it.colwd[p2], didj);
-      wgt = __fma_rn((double)it.roww[s], (double)it.colw[p2], wgt);
+      didj = __fma_rn(rp.wd, cq.wd, didj);
+      wgt = __fma_rn((double)rp.w, (double)cq.w, wgt);
     }
   }
   // runs still open at the last row, then the queue
@@ -259,6 +264,8 @@ __global__ void __launch_bounds__(kDiagWarps * 32, 3) diag_kernel(const __grid_c
     it.colw = A.w + A.off[j];
     it.prei = A.prefix + A.off[i] + i;
     it.prej = A.prefix + A.off[j] + j;
+    it.rowp = A.pack + oi;
+    it.colp = A.pack + oj;
     // Column window |d1 - d2| < lim of every row (the pixel-pair kernel's
     // Polar bound: r^2 >= (d2 - d1)^2 + 2(1 - c) dmin_i dmin_j - err), and
     // from it the diagonals that reach it: delta in [dlo, dhi].

@@ -118,8 +118,8 @@ __device__ __forceinline__ void grid_pass(const PairArgs& A, const SweepItem& it
   const Dest d = it.d;
   const double c = it.c;
   const float ap = it.ap, inv1sqf = A.inv1sqf;
-  const float *rowd = it.rowd, *rowl = it.rowl, *roww = it.roww, *colx = it.colx;
-  const double* rowwd = it.rowwd;
+  const float *rowl = it.rowl, *colx = it.colx;
+  const PixPack* rowp = it.rowp;
   const double4* pre = it.pre;
   const uint16_t* tab = A.gq + (size_t)fi * nbd;  // row r: tab[r * nbd + t]
   // Rows where a run of the pass is non-empty: B[t0 + m] > fj and
@@ -160,8 +160,8 @@ __device__ __forceinline__ void grid_pass(const PairArgs& A, const SweepItem& it
   float x2 = colx[min(b, nj - 1)];
   double2 pwd = *reinterpret_cast<const double2*>(&pre[b]);
   double pl = pre[b].z;
-  RowRaw cR = row_raw(rowd, rowwd, roww, rowl, r0);
-  RowRaw nR = row_raw(rowd, rowwd, roww, rowl, r1);
+  RowRaw cR = row_raw_packed(rowp, rowl, r0);
+  RowRaw nR = row_raw_packed(rowp, rowl, r1);
 #pragma unroll 1
   for (int q = 0; q < iters; ++q, r += P) {
     const bool valid = act && r < g_hi;
@@ -171,7 +171,7 @@ __device__ __forceinline__ void grid_pass(const PairArgs& A, const SweepItem& it
     const double npl = pre[nb].z;
     const int r2 = min(r + 2 * P, g_hi - 1);
     const int nnb = bound(r2);
-    const RowRaw nnR = row_raw(rowd, rowwd, roww, rowl, r2);
+    const RowRaw nnR = row_raw_packed(rowp, rowl, r2);
     const RowV R = row_derive<COORD>(cR, ap, inv1sqf);
     // this lane's boundary: r_perp code of column b (of the last column when
     // b = nj: then it is the code of the last column of the run ending here)

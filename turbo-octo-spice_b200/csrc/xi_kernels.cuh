@@ -63,6 +63,7 @@ struct PairArgs {
   const uint32_t* npix;      // pixels per sightline
   const float* dist_pad;     // padded distances
   const float* loglam_pad;   // padded log10 wavelengths
+  const PixPack* pack;       // padded (distance, weight, w*delta)
   const double* wd;          // w * delta (exact double) per pixel
   const float* w;            // weight per pixel
   const double4* prefix;     // per sightline, N+1 exclusive prefix sums of (wd, w, loglam)

@@ -285,6 +285,7 @@ struct SweepItem {
   const float *rowd, *rowl, *rowx, *roww, *colx;
   const double* rowwd;
   const double4* pre;
+  const PixPack* rowp;  // padded (distance, weight, w*delta) of the rows
 };
 
 // Load work item idx; false when the item belongs to another kernel (z index
@@ -311,6 +312,7 @@ __device__ __forceinline__ bool load_item(const PairArgs& A, unsigned long long 
   const uint64_t oi = A.off[it.i] + (uint64_t)kPad * (it.i + 1);
   const uint64_t oj = A.off[it.j] + (uint64_t)kPad * (it.j + 1);
   it.rowd = A.dist_pad + oi;
+  it.rowp = A.pack + oi;
   it.rowl = A.loglam_pad + oi;
   it.rowx = (COORD == kObs) ? it.rowl : it.rowd;
   it.rowwd = A.wd + A.off[it.i];
@@ -338,6 +340,17 @@ __device__ __forceinline__ RowRaw row_raw(const float* rowd, const double* rowwd
   q.d1 = rowd[r];
   q.wd1 = rowwd[r];
   q.w1 = roww[r];
+  q.l1 = rowl[r];
+  return q;
+}
+
+// The same from the packed row array (one 16-byte load and the loglam).
+__device__ __forceinline__ RowRaw row_raw_packed(const PixPack* rowp, const float* rowl, int r) {
+  const PixPack p = rowp[r];
+  RowRaw q;
+  q.d1 = p.d;
+  q.wd1 = p.wd;
+  q.w1 = p.w;
   q.l1 = rowl[r];
   return q;
 }
