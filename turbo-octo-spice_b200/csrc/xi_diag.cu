@@ -158,7 +158,7 @@ __device__ __forceinline__ void diag_group(const PairArgs& A, const DItem& it, i
   int qn = 0;  // queued runs (the same in every lane)
   double didj = 0.0, wgt = 0.0;
   unsigned rech = 0;
-  unsigned long long n_eval = 0;
+  unsigned n_eval = 0;  // at most one per row of the group
 #pragma unroll 1
   for (int s = s_lo; s < s_hi; ++s) {
     // p2 stays within the 32 sentinels on either side of the padded
@@ -219,7 +219,7 @@ __device__ __forceinline__ void diag_group(const PairArgs& A, const DItem& it, i
     drain(A, it, q, qn, 32, lane);
   }
   drain(A, it, q, 0, qn, lane);
-  stats[0] += n_eval;
+  stats[0] += (unsigned long long)n_eval;
   stats[1] += rech;
 }
 

@@ -161,17 +161,17 @@ __device__ __forceinline__ void grid_pass(const PairArgs& A, const SweepItem& it
   double2 pwd = *reinterpret_cast<const double2*>(&pre[b]);
   double pl = pre[b].z;
   RowRaw cR = row_raw_packed(rowp, rowl, r0);
-  RowRaw nR = row_raw_packed(rowp, rowl, r1);
 #pragma unroll 1
   for (int q = 0; q < iters; ++q, r += P) {
     const bool valid = act && r < g_hi;
-    // loads for the rows ahead
+    // loads for the rows ahead (the row values, broadcast loads that hit in
+    // L1, one row ahead only)
     const float nx2 = colx[min(nb, nj - 1)];
     const double2 npwd = *reinterpret_cast<const double2*>(&pre[nb]);
     const double npl = pre[nb].z;
     const int r2 = min(r + 2 * P, g_hi - 1);
     const int nnb = bound(r2);
-    const RowRaw nnR = row_raw_packed(rowp, rowl, r2);
+    const RowRaw nR = row_raw_packed(rowp, rowl, min(r + P, g_hi - 1));
     const RowV R = row_derive<COORD>(cR, ap, inv1sqf);
     // this lane's boundary: r_perp code of column b (of the last column when
     // b = nj: then it is the code of the last column of the run ending here)
@@ -198,7 +198,6 @@ __device__ __forceinline__ void grid_pass(const PairArgs& A, const SweepItem& it
     pwd = npwd;
     pl = npl;
     cR = nR;
-    nR = nnR;
   }
   if (owner) acc.finish<COORD>(A, d, k);
   stats[0] += n_eval;
