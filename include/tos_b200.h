@@ -380,7 +380,7 @@ tos_status tos_brute_tune(tos_engine* engine, const float* points, size_t n_poin
  * writes the results on the engine's own stream, with no ordering against
  * the caller's streams: the writes that produced the points must be complete
  * (for example the caller's stream synchronised) before the call.  All
- * scratch lives in one static device array of about 8.5 MB that the
+ * scratch lives in one static device array of about 6.5 MB that the
  * library reserves on every GPU that loads it, until the process exits,
  * which limits a call to n_points <= 262144 and nbins <= 4096 (larger
  * requests fail with TOS_ERR_INVALID_ARG).  The first call on a device looks

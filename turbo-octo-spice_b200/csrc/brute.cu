@@ -45,9 +45,8 @@ constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
 constexpr long long kMagicBits = 0x4338000000000000LL;
 
 struct BruteArgs {
-  const float4* pos;      // (x, y, z, 0), n entries
+  const float4* pos;      // (x, y, z, w), n entries
   const double* wd;       // w*delta per point (exact product of the two floats)
-  const double* w;        // w per point
   int n;
   int nbins;
   double min, max, spacing;
@@ -167,7 +166,7 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
     int s0[K];
     double ds[K], ws[K];
     float4 cp[K];
-    double cwd[K], cw[K];
+    double cwd[K];
 #pragma unroll
     for (int m = 0; m < K; ++m) {
       cur[m] = 0xFFFFFFFFu;
@@ -178,28 +177,25 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
 #pragma unroll
     for (int m = 0; m + 1 < K; ++m) {
       cp[m] = make_float4(0.f, 0.f, 0.f, 0.f);
-      cwd[m] = cw[m] = 0.0;
+      cwd[m] = 0.0;
       if (d0 + m < A.n) {
         cp[m] = A.pos[d0 + m];
         cwd[m] = A.wd[d0 + m];
-        cw[m] = A.w[d0 + m];
       }
     }
     int qn = 0;  // queued runs (the same in every lane)
     // the lane's newest column (t + d0 + K - 1) and the row, walked by pointer
     const float4* pj = A.pos + (d0 + K - 1);
     const double* wdj = A.wd + (d0 + K - 1);
-    const double* wj = A.w + (d0 + K - 1);
     const int j_end = A.n - (d0 + K - 1);  // rows t < j_end have the newest column
 #pragma unroll 1
     for (int t = 0; t < t_end; ++t) {
       if (t < j_end) {
         cp[K - 1] = pj[t];
         cwd[K - 1] = wdj[t];
-        cw[K - 1] = wj[t];
       }
       const float4 pi = A.pos[t];
-      const double wdi = A.wd[t], wi = A.w[t];
+      const double wdi = A.wd[t], wi = (double)pi.w;
 #pragma unroll
       for (int m = 0; m < K; ++m) {
         const bool in = t < j_end + (K - 1 - m);  // t + d0 + m < n
@@ -237,14 +233,13 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
         }
         if (in) {
           ds[m] = __fma_rn(wdi, cwd[m], ds[m]);
-          ws[m] = __fma_rn(wi, cw[m], ws[m]);
+          ws[m] = __fma_rn(wi, (double)cp[m].w, ws[m]);
         }
       }
 #pragma unroll
       for (int m = 0; m + 1 < K; ++m) {
         cp[m] = cp[m + 1];
         cwd[m] = cwd[m + 1];
-        cw[m] = cw[m + 1];
       }
     }
     // runs still open: a diagonal's last pair is at row n - 1 - delta, and
@@ -267,12 +262,11 @@ __global__ void __launch_bounds__(kBruteWarpsMax * 32) brute_kernel(BruteArgs A)
   if (lane == 0) atomicAdd(&A.counters[0], n_recheck);
 }
 
-__global__ void k_brute_prep(const float* pts, int n, float4* pos, double* wd, double* w) {
+__global__ void k_brute_prep(const float* pts, int n, float4* pos, double* wd) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const float* p = pts + 5 * (size_t)k;
-    pos[k] = make_float4(p[0], p[1], p[2], 0.f);
+    pos[k] = make_float4(p[0], p[1], p[2], p[4]);
     wd[k] = (double)p[4] * (double)p[3];
-    w[k] = (double)p[4];
   }
 }
 
@@ -446,7 +440,7 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
   cudaStream_t st = e->stream;
   DevBuf<float> d_pts;
   DevBuf<float4> d_pos;
-  DevBuf<double> d_wd, d_w, d_out;
+  DevBuf<double> d_wd, d_out;
   DevBuf<unsigned long long> d_acc, d_misc;
   DevBuf<uint64_t> d_cnt;
   DevBuf<double> d_th;
@@ -456,7 +450,6 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
   TOS_TRY(d_pts.alloc((size_t)n * 5));
   TOS_TRY(d_pos.alloc(n));
   TOS_TRY(d_wd.alloc(n));
-  TOS_TRY(d_w.alloc(n));
   TOS_TRY(d_acc.alloc((size_t)nb2 * kBWin));
   TOS_TRY(d_out.alloc((size_t)nb2 * 2));
   TOS_TRY(d_cnt.alloc(nb2));
@@ -465,12 +458,11 @@ extern "C" tos_status tos_brute_run(tos_engine* e, const float* points, size_t n
                                cudaMemcpyHostToDevice, st));
   TOS_CUDA_TRY(cudaMemsetAsync(d_acc.p, 0, (size_t)nb2 * kBWin * 8, st));
   TOS_CUDA_TRY(cudaMemsetAsync(d_misc.p, 0, 32, st));
-  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_pts.p, n, d_pos.p, d_wd.p, d_w.p);
+  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_pts.p, n, d_pos.p, d_wd.p);
   TOS_CUDA_TRY(cudaGetLastError());
   BruteArgs A{};
   A.pos = d_pos.p;
   A.wd = d_wd.p;
-  A.w = d_w.p;
   brute_args(A, n, nbins, min, max, mwd, mw);
   A.th = d_th.p;
   A.acc = d_acc.p;
@@ -524,7 +516,7 @@ extern "C" tos_status tos_brute_tune(tos_engine* e, const float* points, size_t 
   cudaStream_t st = e->stream;
   DevBuf<float> d_pts;
   DevBuf<float4> d_pos;
-  DevBuf<double> d_wd, d_w, d_th;
+  DevBuf<double> d_wd, d_th;
   DevBuf<unsigned long long> d_acc, d_misc;
   const std::vector<double> th = brute_thresholds(min, max, nbins);  // kept until the stream sync
   TOS_TRY(d_th.alloc(th.size()));
@@ -532,16 +524,14 @@ extern "C" tos_status tos_brute_tune(tos_engine* e, const float* points, size_t 
   TOS_TRY(d_pts.alloc((size_t)n * 5));
   TOS_TRY(d_pos.alloc(n));
   TOS_TRY(d_wd.alloc(n));
-  TOS_TRY(d_w.alloc(n));
   TOS_TRY(d_acc.alloc((size_t)nb2 * kBWin));
   TOS_TRY(d_misc.alloc(4));
   TOS_CUDA_TRY(cudaMemcpyAsync(d_pts.p, points, (size_t)n * 5 * sizeof(float), cudaMemcpyHostToDevice, st));
-  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_pts.p, n, d_pos.p, d_wd.p, d_w.p);
+  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_pts.p, n, d_pos.p, d_wd.p);
   TOS_CUDA_TRY(cudaGetLastError());
   BruteArgs A{};
   A.pos = d_pos.p;
   A.wd = d_wd.p;
-  A.w = d_w.p;
   brute_args(A, n, nbins, min, max, mwd, mw);
   A.th = d_th.p;
   A.acc = d_acc.p;
@@ -600,11 +590,10 @@ constexpr size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 // scratch layout (byte offsets, each 256-byte aligned)
 constexpr size_t kNaPos = 0;                                                  // float4[n]
 constexpr size_t kNaWd = kNaPos + round256(16 * kNoAllocMaxPoints);           // double[n]
-constexpr size_t kNaW = kNaWd + round256(8 * kNoAllocMaxPoints);              // double[n]
-constexpr size_t kNaAcc = kNaW + round256(8 * kNoAllocMaxPoints);             // u64[nbins + 2][kBWin]
+constexpr size_t kNaAcc = kNaWd + round256(8 * kNoAllocMaxPoints);            // u64[nbins + 2][kBWin]
 constexpr size_t kNaTh = kNaAcc + round256(8 * kBWin * (kNoAllocMaxBins + 2));  // double[nbins + 3]
 constexpr size_t kNaMisc = kNaTh + round256(8 * (kNoAllocMaxBins + 3));         // u64[8]
-constexpr size_t kNoAllocBytes = kNaMisc + 256;                               // ~8.5 MB
+constexpr size_t kNoAllocBytes = kNaMisc + 256;                               // ~6.5 MB
 
 // The scratch.  Host code must not pass this name to a kernel: on the host
 // it stands for a host-side shadow, not for the device memory; the device
@@ -686,7 +675,6 @@ extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points
   cudaStream_t st = e->stream;
   float4* pos = (float4*)(S + kNaPos);
   double* wd = (double*)(S + kNaWd);
-  double* w = (double*)(S + kNaW);
   unsigned long long* acc = (unsigned long long*)(S + kNaAcc);
   double* thr = (double*)(S + kNaTh);
   unsigned long long* misc = (unsigned long long*)(S + kNaMisc);  // [0] group counter [1] rechecks
@@ -697,7 +685,7 @@ extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points
   TOS_CUDA_TRY(cudaMemsetAsync(acc, 0, (size_t)nb2 * kBWin * sizeof(unsigned long long), st));
   TOS_CUDA_TRY(cudaMemsetAsync(misc, 0, 8 * sizeof(unsigned long long), st));
   k_brute_bounds<<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(d_points, n, misc + 2, misc + 4);
-  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_points, n, pos, wd, w);
+  k_brute_prep<<<std::min(4096, (n + 255) / 256), 256, 0, st>>>(d_points, n, pos, wd);
   TOS_CUDA_TRY(cudaGetLastError());
   unsigned long long hb[3] = {0, 0, 0};
   TOS_CUDA_TRY(cudaMemcpyAsync(hb, misc + 2, sizeof(hb), cudaMemcpyDeviceToHost, st));
@@ -712,7 +700,6 @@ extern "C" tos_status tos_brute_run_noalloc(tos_engine* e, const float* d_points
   BruteArgs A{};
   A.pos = pos;
   A.wd = wd;
-  A.w = w;
   brute_args(A, n, nbins, min, max, mwd, mw);
   A.th = thr;
   A.acc = acc;

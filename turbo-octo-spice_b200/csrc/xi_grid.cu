@@ -233,7 +233,6 @@ __global__ void __launch_bounds__(kGridThreads, 4) grid_kernel(const __grid_cons
   add_counters(A, lane, stats[0], stats[1], n_taken, 9);
 }
 
-// Persistent launch: as many CTAs as fit on the SMs at once.
 // Persistent launch: `ctas_per_sm` CTAs per SM (0 or above the occupancy
 // limit: as many as fit), or with `max_out` set only that limit.
 template <int COORD, bool MINPOS>
