@@ -163,6 +163,34 @@ tos_status tos_catalog_create_dc(tos_engine* engine, const tos_sightline* los, s
                                  const tos_pixel* pixels, size_t n_pixels, int order, double omega_matter,
                                  tos_catalog** out);
 
+/* One platelist row: the PLATE, RACEN and DECCEN columns (centre in degrees)
+ * that PlateBins reads from the platelist FITS file (PlateBins.h:38-45). */
+typedef struct {
+  int32_t plate;
+  float ra_center, dec_center;
+} tos_plate;
+
+/* tos_catalog_create with the sightlines binned by BOSS plate instead of
+ * HEALPix: PlateBins (PlateBins.h:18-92), what h5healxi builds when its
+ * HEALPix order is 0 (h5healxi.cc:166-174).  A sightline's cell is its
+ * `plate` (cell id group * 2^32 + plate; plate ids must be >= 0).  The
+ * sightlines a primary pairs with are those on the platelist plates whose
+ * centre lies at an angle theta from it with |theta - 1.5 deg| < max_ang
+ * (PlateBins::getBinIndicesWithinRadius, PlateBins.h:73-84; theta = acos of
+ * SkyObject::angularSeparation, as the reference computes it), then the
+ * cos(theta_ij) cut as for HEALPix cells.  That test is a ring, not a disc:
+ * when max_ang < 1.5 deg, plates whose centre is nearer than 1.5 deg -
+ * max_ang are skipped, and their pairs with it are not counted, exactly as
+ * in the reference.  A plate id listed twice keeps its last row (the map
+ * assignment of PlateBins.h:44); sightlines on a plate absent from the
+ * platelist are primaries but nobody's neighbours.  omega_matter: 0 to keep
+ * the pixels' distances, else as tos_catalog_create_dc.  tos_xi_run_jackknife
+ * and tos_xi_jackknife (HEALPix regions) return TOS_ERR_UNSUPPORTED on such
+ * a catalogue. */
+tos_status tos_catalog_create_plates(tos_engine* engine, const tos_sightline* los, size_t n_los,
+                                     const tos_pixel* pixels, size_t n_pixels, const tos_plate* platelist,
+                                     size_t n_plates, double omega_matter, tos_catalog** out);
+
 /* The catalogue's per-pixel comoving distances (float, in the compact order
  * of the catalogue: the pixels of sightline 0, then of sightline 1, ...). */
 tos_status tos_catalog_distances(const tos_catalog* catalog, float* out, size_t capacity);
@@ -172,9 +200,11 @@ void tos_catalog_destroy(tos_catalog* catalog);
 tos_status tos_catalog_num_cells(const tos_catalog* catalog, size_t* n_cells);
 /* Occupied cell ids in ascending order — the key order of
  * XiEstimator::skybin_xis_ (XiEstimator.h:78) and of the subsample files.
- * A cell id is group * 2^32 + HEALPix pixel (the pixel alone in group 0). */
+ * A cell id is group * 2^32 + HEALPix pixel (the pixel alone in group 0),
+ * or group * 2^32 + plate in a catalogue of tos_catalog_create_plates. */
 tos_status tos_catalog_cells(const tos_catalog* catalog, int64_t* cell_ids, size_t capacity);
-/* Cell id of each sightline (HealpixBins::ang2pix, HealpixBins.h:58-66). */
+/* Cell id of each sightline (HealpixBins::ang2pix, HealpixBins.h:58-66, or
+ * its plate, PlateBins.h:59). */
 tos_status tos_catalog_sightline_cells(const tos_catalog* catalog, int64_t* cells, size_t capacity);
 /* Number of distinct sightline groups, and their ids in ascending order (the
  * row order of a TOS_XI_PER_GROUP result). */

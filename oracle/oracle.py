@@ -25,7 +25,7 @@ XIBIN_DTYPE = np.dtype([("didj", "<f8"), ("di", "<f8"), ("dj", "<f8"), ("wgt", "
 class OrcStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("num_sightline_pairs_used", "num_pixels", "num_pixel_pairs",
                                           "num_pixel_pairs_used", "num_index_overflow")] + [
-        ("max_ang", C.c_double), ("cos_max_ang", C.c_double)]
+        ("max_ang", C.c_double), ("cos_max_ang", C.c_double), ("num_sightline_pairs", C.c_uint64)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -49,6 +49,9 @@ def lib(kind: str = "strict") -> C.CDLL:
         L.orc_xi.argtypes = [vp, vp, vp, vp, sz, vp, i32, i32, vp, dbl, i32, i32, vp, sz, vp, vp, vp,
                              C.POINTER(OrcStats)]
         L.orc_xi.restype = C.c_long
+        L.orc_xi_plates.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp, vp, vp, sz, i32, vp, dbl, i32, i32, vp, sz,
+                                    vp, vp, vp, C.POINTER(OrcStats)]
+        L.orc_xi_plates.restype = C.c_long
         L.orc_cell_costs.argtypes = [vp, vp, vp, sz, i32, i32, vp, dbl, vp]
         L.orc_cell_costs.restype = C.c_long
         L.orc_brute.argtypes = [vp, sz, dbl, dbl, i32, i32, vp, vp, vp]
@@ -91,6 +94,46 @@ def xi(sightlines, pixels, order: int, coord: int, axes, scale: float, mode: int
         nthreads = os.cpu_count() or 1
     r = L.orc_xi(_p(ra), _p(dec), _p(off), _p(npx), len(ra), _p(px), order, coord, _p(axes), scale, mode,
                  nthreads, _p(sub), 0 if sub is None else len(sub), _p(bins), _p(cells), _p(ids), C.byref(st))
+    if r < 0:
+        raise ValueError("oracle rejected the input")
+    return bins, cells, ids, st.as_dict()
+
+
+def _platelist(platelist):
+    """(plate ids int32, RACEN float32, DECCEN float32) of a platelist given as
+    a structured array with fields plate, ra_center, dec_center (degrees)."""
+    return (np.ascontiguousarray(platelist["plate"], dtype=np.int32),
+            np.ascontiguousarray(platelist["ra_center"], dtype=np.float32),
+            np.ascontiguousarray(platelist["dec_center"], dtype=np.float32))
+
+
+def xi_plates(sightlines, pixels, platelist, coord: int, axes, scale: float, mode: int = 1, nthreads: int = 0,
+              cell_subset=None, subsamples: bool = False, kind: str = "strict"):
+    """Oracle pair count with sightlines binned by their plate (PlateBins):
+    cells are the sightlines' plate ids, neighbours the platelist plates
+    whose centres pass PlateBins' ring test.  Returns (bins, cells or None,
+    cell_ids, stats); stats also has num_sightline_pairs (candidates)."""
+    L = lib(kind)
+    ra = np.ascontiguousarray(sightlines["ra"], dtype=np.float64)
+    dec = np.ascontiguousarray(sightlines["dec"], dtype=np.float64)
+    plate = np.ascontiguousarray(sightlines["plate"], dtype=np.int32)
+    off = np.ascontiguousarray(sightlines["pixel_offset"], dtype=np.uint64)
+    npx = np.ascontiguousarray(sightlines["num_pixels"], dtype=np.uint32)
+    px = np.ascontiguousarray(pixels)
+    axes = np.ascontiguousarray(axes, dtype=np.float64)
+    lp, lra, ldec = _platelist(platelist)
+    nb = int(axes[2] * axes[5] * axes[8])
+    ncells = len(np.unique(plate))
+    bins = np.zeros(nb, dtype=XIBIN_DTYPE)
+    cells = np.zeros((ncells, nb), dtype=XIBIN_DTYPE) if subsamples else None
+    ids = np.zeros(ncells, dtype=np.int64)
+    sub = None if cell_subset is None else np.ascontiguousarray(cell_subset, dtype=np.uint32)
+    st = OrcStats()
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    r = L.orc_xi_plates(_p(ra), _p(dec), _p(plate), _p(off), _p(npx), len(ra), _p(px), _p(lp), _p(lra), _p(ldec),
+                        len(lp), coord, _p(axes), scale, mode, nthreads, _p(sub), 0 if sub is None else len(sub),
+                        _p(bins), _p(cells), _p(ids), C.byref(st))
     if r < 0:
         raise ValueError("oracle rejected the input")
     return bins, cells, ids, st.as_dict()
@@ -172,6 +215,9 @@ def ref_lib(kind: str = "strict") -> C.CDLL:
             L.tosref_xi.argtypes = [vp, vp, vp, vp, sz, vp, i32, i32, vp, dbl, i32, vp, sz, vp, vp, vp, vp, sz,
                                     vp, vp, vp, C.c_char_p, sz]
             L.tosref_xi.restype = C.c_long
+            L.tosref_xi_plates.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp, vp, vp, sz, i32, vp, dbl, i32, vp, sz,
+                                           vp, vp, vp, vp, sz, vp, vp, vp, C.c_char_p, sz]
+            L.tosref_xi_plates.restype = C.c_long
             L.tosref_radec2pix.argtypes = [i32, dbl, dbl]
             L.tosref_radec2pix.restype = C.c_int64
             L.tosref_max_centre_distance.argtypes = [i32, vp, sz, C.POINTER(C.c_double)]
@@ -215,6 +261,43 @@ def ref_xi(sightlines, pixels, order: int, coord: int, axes, scale: float, nthre
     n = L.tosref_xi(_p(ra), _p(dec), _p(off), _p(npx), len(ra), _p(px), order, coord, _p(axes), scale, nthreads,
                     _p(sub), 0 if sub is None else len(sub), _p(bins), _p(final), _p(cells), _p(ids), cap,
                     _p(cnt), _p(ang), C.byref(secs), err, 512)
+    if n < 0:
+        raise ValueError("reference XiEstimator failed: " + err.value.decode())
+    st = {k: int(v) for k, v in zip(REF_COUNTERS, cnt)}
+    st["max_ang"], st["cos_max_ang"] = float(ang[0]), float(ang[1])
+    st["run_seconds"] = secs.value
+    return bins, final, (cells[:n] if cells is not None else None), ids[:n], st
+
+
+def ref_xi_plates(sightlines, pixels, platelist, coord: int, axes, scale: float, nthreads: int = 0,
+                  cell_subset=None, subsamples: bool = False, kind: str = "strict"):
+    """ref_xi with the reference's PlateBins (cell ids = plate ids; the
+    platelist is handed to PlateBins' own constructor)."""
+    L = ref_lib(kind)
+    ra = np.ascontiguousarray(sightlines["ra"], dtype=np.float64)
+    dec = np.ascontiguousarray(sightlines["dec"], dtype=np.float64)
+    plate = np.ascontiguousarray(sightlines["plate"], dtype=np.int32)
+    off = np.ascontiguousarray(sightlines["pixel_offset"], dtype=np.uint64)
+    npx = np.ascontiguousarray(sightlines["num_pixels"], dtype=np.uint32)
+    px = np.ascontiguousarray(pixels)
+    axes = np.ascontiguousarray(axes, dtype=np.float64)
+    lp, lra, ldec = _platelist(platelist)
+    nb = int(axes[2] * axes[5] * axes[8])
+    sub = None if cell_subset is None else np.ascontiguousarray(cell_subset, dtype=np.int64)
+    cap = len(sub) if sub is not None else len(ra)
+    bins = np.zeros(nb, dtype=XIBIN_DTYPE)
+    final = np.zeros(nb, dtype=XIBIN_DTYPE)
+    cells = np.zeros((cap, nb), dtype=XIBIN_DTYPE) if subsamples else None
+    ids = np.zeros(cap, dtype=np.int64)
+    cnt = np.zeros(5, dtype=np.uint64)
+    ang = np.zeros(2)
+    err = C.create_string_buffer(512)
+    secs = C.c_double()
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    n = L.tosref_xi_plates(_p(ra), _p(dec), _p(plate), _p(off), _p(npx), len(ra), _p(px), _p(lp), _p(lra), _p(ldec),
+                           len(lp), coord, _p(axes), scale, nthreads, _p(sub), 0 if sub is None else len(sub),
+                           _p(bins), _p(final), _p(cells), _p(ids), cap, _p(cnt), _p(ang), C.byref(secs), err, 512)
     if n < 0:
         raise ValueError("reference XiEstimator failed: " + err.value.decode())
     st = {k: int(v) for k, v in zip(REF_COUNTERS, cnt)}

@@ -22,19 +22,25 @@
  *    of every signed term (didj, di, dj), the scale against which a bin whose
  *    signed sum cancels is judged;
  *  - HealpixBins::ang2pix (HealpixBins.h:58-72) with RING numbering
- *    (Gorski et al. 2005) for the cell of each sightline;
+ *    (Gorski et al. 2005) for the cell of each sightline, or, in
+ *    orc_xi_plates, PlateBins (PlateBins.h:18-92): cells keyed by plate and
+ *    the neighbour plates of its ring test |theta - 1.5 deg| < max_ang;
  *  - the brute-force estimator's histogram (gpu/brute.cu:40-52) with the FP64
  *    separation of bucketxi (src/bucketxi.cc:79-98).
  * The neighbour search is a declination band scan instead of HEALPix
  * query_disc_inclusive: both return every sightline within max_ang, and the
  * exact cos cut decides, so the accepted pairs are the same.
  *
- * Parity unpinned: the reference ships no expected outputs for this path, and
- * its own code cannot be built here (XiEstimator.cc needs boost, likely,
- * Healpix_cxx and cosmo).  This restatement is checked against a literal
- * transcription of the reference's loop (tests/ref_loop.py), hand-built
- * known answers at bin edges, and HEALPix known pixels; tests/golden holds
- * fixtures generated from it (tests/golden/make_golden.py).
+ * Parity pinned: the reference ships no expected outputs for this path, so
+ * its own XiEstimator.cc, grid classes, ThreadPool.cc and PlateBins.h are
+ * compiled unchanged against stand-in headers (oracle/ref_harness.cc,
+ * oracle/refshim, `make -C oracle ref`), and the tests compare this
+ * restatement with that build: the golden fixtures of tests/golden hold its
+ * outputs (tests/golden/make_golden.py), and the live build is compared
+ * wherever it is present.  Mode 0 reproduces it bit for bit.  Also checked
+ * against a literal transcription of the reference's loop
+ * (tests/ref_loop.py), hand-built known answers at bin edges, and HEALPix
+ * known pixels.
  *
  * static_cast<unsigned>(double) is reproduced as the x86-64 code of the
  * reference build computes it (cvttsd2si into 64 bits, low 32 bits kept).
@@ -52,6 +58,7 @@ typedef struct {
   uint64_t num_sightline_pairs_used, num_pixels, num_pixel_pairs, num_pixel_pairs_used,
       num_index_overflow;
   double max_ang, cos_max_ang;
+  uint64_t num_sightline_pairs; /* candidates j > i in neighbour cells: plate cells only (0 otherwise) */
 } orc_stats;
 
 enum { ORC_POLAR = 0, ORC_CARTESIAN = 1, ORC_OBSERVING = 2 };
@@ -147,12 +154,18 @@ typedef struct {
   /* cells */
   const uint32_t* cell_start; /* CSR over members */
   const uint32_t* members;
+  /* plate cells (orc_xi_plates): the platelist, one entry per plate id in
+   * ascending id order, its centres' sines and cosines, and the cell of each
+   * entry (-1: no sightline on that plate) */
+  size_t n_plates;
+  const double *psd, *pcd, *psr, *pcr;
+  const int64_t* plate_cell;
   /* run */
   orc_grid g;
   double cos_max;
   int mode;
   orc_xibin* cell_bins; /* [n_cells][ntotal] */
-  uint64_t* cell_ctr;   /* [n_cells][4]: used pairs, pixel pairs, pixel pairs used, overflow */
+  uint64_t* cell_ctr;   /* [n_cells][5]: used pairs, pixel pairs, pixel pairs used, overflow, candidates */
   const uint32_t* todo; /* cells to process */
   size_t n_todo;
   size_t next;
@@ -268,9 +281,48 @@ static uint64_t pixel_pairs(const orc_job* J, uint32_t a, uint32_t b, double c, 
   return used;
 }
 
+/* One accepted-or-not candidate pair (i, j), j > i (XiEstimator.cc:141-151). */
+static void candidate(orc_job* J, uint32_t i, uint32_t j, orc_xibin* xi, uint64_t* ctr) {
+  const double c = J->sd[i] * J->sd[j] + J->cd[i] * J->cd[j] * (J->sr[i] * J->sr[j] + J->cr[i] * J->cr[j]);
+  ctr[4] += 1;
+  if (c <= J->cos_max) return;
+  ctr[0] += 1;
+  ctr[1] += (uint64_t)J->npix[i] * J->npix[j];
+  ctr[2] += pixel_pairs(J, i, j, c, xi, &ctr[3]);
+}
+
+/* Plate cells: PlateBins::getBinIndicesWithinRadius (PlateBins.h:73-84)
+ * takes every platelist plate, in ascending plate id, whose centre's angular
+ * separation from the primary is within max_ang of 1.5 degrees:
+ * |acos(cos_sep) - 1.5 deg| < max_ang; plates without sightlines are skipped
+ * (XiEstimator.cc:136-137), every sightline j > i of the others is a
+ * candidate. */
+static void plate_task(orc_job* J, uint32_t cell, orc_xibin* xi, uint64_t* ctr) {
+  const double deg2rad = (atan(1.0) * 4) / 180.0; /* constants.h:12-13 */
+  const double ring = 1.5 * deg2rad;
+  for (uint32_t q = J->cell_start[cell]; q < J->cell_start[cell + 1]; ++q) {
+    const uint32_t i = J->members[q];
+    for (size_t k = 0; k < J->n_plates; ++k) {
+      const double cs = J->sd[i] * J->psd[k] + J->cd[i] * J->pcd[k] * (J->sr[i] * J->psr[k] + J->cr[i] * J->pcr[k]);
+      if (!(fabs(acos(cs) - ring) < J->g.max_ang)) continue;
+      if (J->plate_cell[k] < 0) continue;
+      const uint32_t nc = (uint32_t)J->plate_cell[k];
+      for (uint32_t m = J->cell_start[nc]; m < J->cell_start[nc + 1]; ++m) {
+        const uint32_t j = J->members[m];
+        if (j <= i) continue;
+        candidate(J, i, j, xi, ctr);
+      }
+    }
+  }
+}
+
 static void skybin_task(orc_job* J, uint32_t cell) {
   orc_xibin* xi = J->cell_bins + (size_t)cell * J->g.ntotal;
-  uint64_t* ctr = J->cell_ctr + 4 * (size_t)cell;
+  uint64_t* ctr = J->cell_ctr + 5 * (size_t)cell;
+  if (J->plate_cell) {
+    plate_task(J, cell, xi, ctr);
+    return;
+  }
   const double lim = J->g.max_ang + 1e-9;
   for (uint32_t q = J->cell_start[cell]; q < J->cell_start[cell + 1]; ++q) {
     const uint32_t i = J->members[q];
@@ -317,6 +369,60 @@ static int cmp_kvi(const void* x, const void* y) {
   const kvi *a = (const kvi*)x, *b = (const kvi*)y;
   if (a->key != b->key) return (a->key > b->key) - (a->key < b->key);
   return (a->idx > b->idx) - (a->idx < b->idx);
+}
+
+/* Runs the tasks of the chosen cells (every cell when cell_subset is NULL)
+ * in nthreads threads, merges the cells in ascending order
+ * (xi_finalize_task, XiEstimator.cc:298-305) and fills the outputs.
+ * Returns the number of occupied cells. */
+static long run_cells(orc_job* J, size_t nc, const int64_t* cell_ids, const uint32_t* cell_subset,
+                      size_t n_subset, int nthreads, orc_xibin* out_bins, orc_xibin* out_cells,
+                      int64_t* out_cell_ids, orc_stats* stats) {
+  J->cell_bins = (orc_xibin*)calloc((size_t)nc * J->g.ntotal, sizeof(orc_xibin));
+  J->cell_ctr = (uint64_t*)calloc(5 * nc, sizeof(uint64_t));
+  uint32_t* todo = (uint32_t*)malloc(4 * (nc ? nc : 1) + 4 * n_subset);
+  if (cell_subset) {
+    for (size_t k = 0; k < n_subset; ++k) todo[k] = cell_subset[k];
+    J->n_todo = n_subset;
+  } else {
+    for (size_t k = 0; k < nc; ++k) todo[k] = (uint32_t)k;
+    J->n_todo = nc;
+  }
+  J->todo = todo;
+  J->next = 0;
+  pthread_mutex_init(&J->mu, NULL);
+  if (nthreads < 1) nthreads = 1;
+  pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
+  for (int t = 0; t < nthreads; ++t) pthread_create(&th[t], NULL, worker, J);
+  for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+  free(th);
+  pthread_mutex_destroy(&J->mu);
+  memset(out_bins, 0, sizeof(orc_xibin) * J->g.ntotal);
+  orc_stats st;
+  memset(&st, 0, sizeof st);
+  for (size_t c = 0; c < nc; ++c) {
+    const orc_xibin* x = J->cell_bins + c * J->g.ntotal;
+    for (uint32_t b = 0; b < J->g.ntotal; ++b) {
+      out_bins[b].didj += x[b].didj; out_bins[b].di += x[b].di; out_bins[b].dj += x[b].dj;
+      out_bins[b].wgt += x[b].wgt; out_bins[b].wi += x[b].wi; out_bins[b].wj += x[b].wj;
+      out_bins[b].z += x[b].z; out_bins[b].num_pairs += x[b].num_pairs;
+    }
+    st.num_sightline_pairs_used += J->cell_ctr[5 * c];
+    st.num_pixel_pairs += J->cell_ctr[5 * c + 1];
+    st.num_pixel_pairs_used += J->cell_ctr[5 * c + 2];
+    st.num_index_overflow += J->cell_ctr[5 * c + 3];
+    st.num_sightline_pairs += J->cell_ctr[5 * c + 4];
+  }
+  for (size_t k = 0; k < J->n_todo; ++k)
+    for (uint32_t q = J->cell_start[todo[k]]; q < J->cell_start[todo[k] + 1]; ++q)
+      st.num_pixels += J->npix[J->members[q]];
+  st.max_ang = J->g.max_ang;
+  st.cos_max_ang = J->cos_max;
+  if (out_cells) memcpy(out_cells, J->cell_bins, sizeof(orc_xibin) * nc * J->g.ntotal);
+  if (out_cell_ids) memcpy(out_cell_ids, cell_ids, 8 * nc);
+  if (stats) *stats = st;
+  free(J->cell_bins); free(J->cell_ctr); free(todo);
+  return (long)nc;
 }
 
 /*
@@ -371,50 +477,84 @@ long orc_xi(const double* ra, const double* dec, const uint64_t* off, const uint
   cell_start[nc] = (uint32_t)n_los;
   free(cs);
   J.cell_start = cell_start; J.members = members;
-  J.cell_bins = (orc_xibin*)calloc((size_t)nc * J.g.ntotal, sizeof(orc_xibin));
-  J.cell_ctr = (uint64_t*)calloc(4 * nc, sizeof(uint64_t));
-  uint32_t* todo = (uint32_t*)malloc(4 * nc);
-  if (cell_subset) {
-    for (size_t k = 0; k < n_subset; ++k) todo[k] = cell_subset[k];
-    J.n_todo = n_subset;
-  } else {
-    for (size_t k = 0; k < nc; ++k) todo[k] = (uint32_t)k;
-    J.n_todo = nc;
-  }
-  J.todo = todo;
-  pthread_mutex_init(&J.mu, NULL);
-  if (nthreads < 1) nthreads = 1;
-  pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
-  for (int t = 0; t < nthreads; ++t) pthread_create(&th[t], NULL, worker, &J);
-  for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
-  free(th);
-  pthread_mutex_destroy(&J.mu);
-  /* merge in ascending cell order (xi_finalize_task) */
-  memset(out_bins, 0, sizeof(orc_xibin) * J.g.ntotal);
-  orc_stats st;
-  memset(&st, 0, sizeof st);
-  for (size_t c = 0; c < nc; ++c) {
-    const orc_xibin* x = J.cell_bins + c * J.g.ntotal;
-    for (uint32_t b = 0; b < J.g.ntotal; ++b) {
-      out_bins[b].didj += x[b].didj; out_bins[b].di += x[b].di; out_bins[b].dj += x[b].dj;
-      out_bins[b].wgt += x[b].wgt; out_bins[b].wi += x[b].wi; out_bins[b].wj += x[b].wj;
-      out_bins[b].z += x[b].z; out_bins[b].num_pairs += x[b].num_pairs;
-    }
-    st.num_sightline_pairs_used += J.cell_ctr[4 * c];
-    st.num_pixel_pairs += J.cell_ctr[4 * c + 1];
-    st.num_pixel_pairs_used += J.cell_ctr[4 * c + 2];
-    st.num_index_overflow += J.cell_ctr[4 * c + 3];
-  }
-  for (size_t k = 0; k < J.n_todo; ++k)
-    for (uint32_t q = cell_start[todo[k]]; q < cell_start[todo[k] + 1]; ++q) st.num_pixels += npix[members[q]];
-  st.max_ang = J.g.max_ang;
-  st.cos_max_ang = J.cos_max;
-  if (out_cells) memcpy(out_cells, J.cell_bins, sizeof(orc_xibin) * nc * J.g.ntotal);
-  if (out_cell_ids) memcpy(out_cell_ids, cell_ids, 8 * nc);
-  if (stats) *stats = st;
+  const long r = run_cells(&J, nc, cell_ids, cell_subset, n_subset, nthreads, out_bins, out_cells, out_cell_ids,
+                           stats);
   free(trig); free(by_dec); free(dec_sorted); free(members); free(cell_start); free(cell_ids);
-  free(J.cell_bins); free(J.cell_ctr); free(todo);
-  return (long)nc;
+  return r;
+}
+
+/*
+ * orc_xi with the sightlines binned by BOSS plate (PlateBins, PlateBins.h:18-92):
+ * plate[s] is sightline s's cell, cells ascending by plate id (the key order
+ * of skybin_xis_); the platelist gives n_list rows of plate id and centre
+ * (RACEN, DECCEN in degrees, as read from the platelist FITS file,
+ * PlateBins.h:38-45).  A plate id listed twice keeps its last row (the
+ * std::map assignment of PlateBins.h:44).  Cell ids are plate ids.
+ */
+long orc_xi_plates(const double* ra, const double* dec, const int32_t* plate, const uint64_t* off,
+                   const uint32_t* npix, size_t n_los, const orc_pixel* px, const int32_t* list_plate,
+                   const float* list_racen, const float* list_deccen, size_t n_list, int coord, const double* axes,
+                   double scale, int mode, int nthreads, const uint32_t* cell_subset, size_t n_subset,
+                   orc_xibin* out_bins, orc_xibin* out_cells, int64_t* out_cell_ids, orc_stats* stats) {
+  if (n_los == 0 || coord < 0 || coord > 2) return -1;
+  orc_job J;
+  memset(&J, 0, sizeof J);
+  make_grid(&J.g, coord, axes, scale);
+  J.cos_max = cos(J.g.max_ang);
+  J.mode = mode;
+  J.off = off;
+  J.npix = npix;
+  J.px = px;
+  J.n_los = n_los;
+  J.dec = dec;
+  double* trig = (double*)malloc(sizeof(double) * 4 * n_los);
+  double* sd = trig; double* cd = trig + n_los; double* sr = trig + 2 * n_los; double* cr = trig + 3 * n_los;
+  for (size_t s = 0; s < n_los; ++s) {
+    sd[s] = sin(dec[s]); cd[s] = cos(dec[s]); sr[s] = sin(ra[s]); cr[s] = cos(ra[s]);
+  }
+  J.sd = sd; J.cd = cd; J.sr = sr; J.cr = cr;
+  /* cells: sightlines by (plate, index) */
+  kvi* cs = (kvi*)malloc(sizeof(kvi) * n_los);
+  for (size_t s = 0; s < n_los; ++s) { cs[s].key = plate[s]; cs[s].idx = (uint32_t)s; }
+  qsort(cs, n_los, sizeof(kvi), cmp_kvi);
+  uint32_t* members = (uint32_t*)malloc(4 * n_los);
+  uint32_t* cell_start = (uint32_t*)malloc(4 * (n_los + 1));
+  int64_t* cell_ids = (int64_t*)malloc(8 * n_los);
+  size_t nc = 0;
+  for (size_t s = 0; s < n_los; ++s) {
+    if (s == 0 || cs[s].key != cs[s - 1].key) { cell_start[nc] = (uint32_t)s; cell_ids[nc] = cs[s].key; ++nc; }
+    members[s] = cs[s].idx;
+  }
+  cell_start[nc] = (uint32_t)n_los;
+  free(cs);
+  J.cell_start = cell_start; J.members = members;
+  /* the platelist: ascending plate id, the last row of a repeated id */
+  kvi* pl = (kvi*)malloc(sizeof(kvi) * (n_list ? n_list : 1));
+  for (size_t k = 0; k < n_list; ++k) { pl[k].key = list_plate[k]; pl[k].idx = (uint32_t)k; }
+  qsort(pl, n_list, sizeof(kvi), cmp_kvi);
+  double* ptrig = (double*)malloc(sizeof(double) * 4 * (n_list ? n_list : 1));
+  int64_t* pcell = (int64_t*)malloc(8 * (n_list ? n_list : 1));
+  const double deg2rad = (atan(1.0) * 4) / 180.0;
+  size_t np = 0;
+  for (size_t k = 0; k < n_list; ++k) {
+    if (k + 1 < n_list && pl[k + 1].key == pl[k].key) continue; /* a later row of the same plate wins */
+    const uint32_t r = pl[k].idx;
+    const double pra = list_racen[r] * deg2rad, pdec = list_deccen[r] * deg2rad;
+    ptrig[np] = sin(pdec); ptrig[n_list + np] = cos(pdec);
+    ptrig[2 * n_list + np] = sin(pra); ptrig[3 * n_list + np] = cos(pra);
+    pcell[np] = -1;
+    for (size_t c = 0; c < nc; ++c)
+      if (cell_ids[c] == pl[k].key) pcell[np] = (int64_t)c;
+    ++np;
+  }
+  free(pl);
+  J.n_plates = np;
+  J.psd = ptrig; J.pcd = ptrig + n_list; J.psr = ptrig + 2 * n_list; J.pcr = ptrig + 3 * n_list;
+  J.plate_cell = pcell;
+  const long r = run_cells(&J, nc, cell_ids, cell_subset, n_subset, nthreads, out_bins, out_cells, out_cell_ids,
+                           stats);
+  free(trig); free(ptrig); free(pcell); free(members); free(cell_start); free(cell_ids);
+  return r;
 }
 
 /* Number of occupied cells and, per occupied cell (ascending id), the pixel

@@ -28,6 +28,28 @@ def small_catalog(n=120, seed=11, size_deg=3.0, max_pixels=None):
     return los, px, meta
 
 
+def plate_catalog(n=90, seed=17, size_deg=6.0, max_pixels=48, spacing_deg=2.0):
+    """A small catalogue on BOSS-like plates (synth.plate_tiling) with the
+    platelist cases PlateBins meets: a plate listed twice (its second row,
+    with a moved centre, is the one kept), a listed plate without sightlines
+    and three sightlines on a plate missing from the platelist.  Returns
+    (sightlines, pixels, platelist, meta)."""
+    los, px, meta = small_catalog(n=n, seed=seed, size_deg=size_deg, max_pixels=max_pixels)
+    los, plates = synth.plate_tiling(los, spacing_deg)
+    used = np.unique(los["plate"])
+    dup = plates[plates["plate"] == used[1]].copy()  # moved far enough to change the count
+    dup["ra_center"] += np.float32(1.0)
+    dup["dec_center"] -= np.float32(0.8)
+    empty = np.zeros(1, dtype=plates.dtype)
+    empty["plate"] = 9000
+    empty["ra_center"] = plates["ra_center"][0]
+    empty["dec_center"] = plates["dec_center"][0]
+    plates = np.concatenate([plates, dup, empty])
+    los = los.copy()
+    los["plate"][[1, 5, 9]] = 8999  # not in the platelist
+    return los, px, plates, meta
+
+
 def as_matrix(bins):
     """XiBin structured array -> (n, 8) float64 with the count in column 7."""
     m = np.zeros((len(bins), 8))

@@ -148,3 +148,26 @@ def test_oracle_reproduces_golden(fixture):
     assert np.array_equal(cells["num_pairs"], z["cell_num_pairs"])
     for f in FIELDS:
         np.testing.assert_allclose(bins[f], z[f], rtol=1e-12, atol=0)
+
+
+def test_plate_ring_covers_the_disc_above_1p5_degrees():
+    """PlateBins' neighbour test |theta - 1.5 deg| < max_ang holds for every
+    plate with a sightline within max_ang when max_ang > 1.5 deg and every
+    sightline lies within 1.5 deg of its plate's centre: then plate cells
+    bin the same pairs as HEALPix cells.  Below 1.5 deg the ring skips plates
+    whose centre is nearer than 1.5 deg - max_ang, and pairs are lost."""
+    from helpers import GRIDS, small_catalog
+    from tos_b200 import synth
+    los, px, meta = small_catalog(n=120, seed=9, size_deg=6.0, max_pixels=24)
+    los, plates = synth.plate_tiling(los, 2.0)
+    g = GRIDS["cartesian"]
+    for factor, same in ((1.0, True), (4.0, False)):
+        scale = factor * meta["scale"]
+        hb, _, _, hst = oracle.xi(los, px, 6, g.type, g.axes_array(), scale, mode=1, nthreads=4)
+        pb, _, _, pst = oracle.xi_plates(los, px, plates, g.type, g.axes_array(), scale, mode=1, nthreads=4)
+        assert (hst["max_ang"] > math.radians(1.5)) == same
+        if same:
+            assert np.array_equal(pb["num_pairs"], hb["num_pairs"])
+            assert pst["num_sightline_pairs_used"] == hst["num_sightline_pairs_used"]
+        else:
+            assert 0 < pb["num_pairs"].sum() < hb["num_pairs"].sum()

@@ -153,3 +153,50 @@ def test_disc_superset_bound():
     for order in (3, 6):
         worst, bound = oracle.ref_max_centre_distance(order, v)
         assert worst < 0.8 * bound, (order, worst, bound)
+
+
+# ---- PlateBins (sky cells = BOSS plates)
+
+def test_oracle_reproduces_reference_plate_fixture():
+    """The plate fixture: a platelist with a repeated plate id, a plate
+    without sightlines and sightlines on an unlisted plate, at a maximum
+    angle below 1.5 degrees (PlateBins' ring test skips nearby plates)."""
+    z = _load("golden_plates_cartesian")
+    los, px, plates, axes = z["sightlines"], z["pixels"], z["platelist"], z["axes"]
+    coord, scale = int(z["coord"]), float(z["scale"])
+    b0, c0, ids, st = oracle.xi_plates(los, px, plates, coord, axes, scale, mode=0, nthreads=4, subsamples=True)
+    assert np.array_equal(b0["num_pairs"], z["ref_num_pairs"])
+    assert np.array_equal(ids, z["ref_cell_ids"])
+    assert np.array_equal(c0["num_pairs"], z["ref_cell_num_pairs"])
+    for f in FIELDS:
+        assert np.array_equal(b0[f], z["ref_" + f]), f
+    cnt = z["ref_counters"]
+    assert st["num_sightline_pairs"] == cnt[0] and st["num_sightline_pairs_used"] == cnt[1]
+    assert st["num_pixels"] == cnt[2] and st["num_pixel_pairs"] == cnt[3] and st["num_pixel_pairs_used"] == cnt[4]
+    assert z["ref_max_ang"][0] < math.radians(1.5)
+    b1 = oracle.xi_plates(los, px, plates, coord, axes, scale, mode=1, nthreads=4)[0]
+    assert np.array_equal(b1["num_pairs"], z["ref_num_pairs"])
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["cartesian", "polar", "observing"])
+@pytest.mark.parametrize("scale_factor", [1.0, 4.0])
+def test_plate_bins_match_live_reference(name, scale_factor):
+    """The oracle's plate cells against the reference's own PlateBins (its
+    constructor reading the platelist through the CCfits stand-in): the
+    cells, every counter and the sums bit for bit."""
+    from helpers import plate_catalog
+    los, px, plates, meta = plate_catalog(n=80, seed=5, size_deg=7.0, max_pixels=32)
+    g = GRIDS[name]
+    scale = scale_factor * meta["scale"]
+    rb, _, rc, rids, rst = oracle.ref_xi_plates(los, px, plates, g.type, g.axes_array(), scale, nthreads=4,
+                                                subsamples=True)
+    ob, oc, oids, ost = oracle.xi_plates(los, px, plates, g.type, g.axes_array(), scale, mode=0, nthreads=4,
+                                         subsamples=True)
+    assert rst["num_pixel_pairs_used"] > 0
+    for k in ("num_sightline_pairs", "num_sightline_pairs_used", "num_pixels", "num_pixel_pairs",
+              "num_pixel_pairs_used"):
+        assert ost[k] == rst[k], k
+    assert np.array_equal(oids, rids)
+    assert np.array_equal(oc["num_pairs"], rc["num_pairs"])
+    assert_same_as_reference(ob, rb, exact=True)

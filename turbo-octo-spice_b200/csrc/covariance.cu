@@ -234,6 +234,8 @@ extern "C" tos_status tos_xi_jackknife(tos_engine* e, tos_catalog* cat, int regi
   std::lock_guard<std::mutex> run_lock(cat->run_mu);  // the sums of cat->run stay put
   TOS_TRY(check_last_run(e, cat));
   if (!n_regions) return fail(TOS_ERR_INVALID_ARG, "n_regions is null");
+  if (cat->plates)
+    return fail(TOS_ERR_UNSUPPORTED, "jackknife regions are HEALPix pixels: a plate catalogue has none");
   if (region_order < 0 || region_order > cat->order)
     return fail(TOS_ERR_INVALID_ARG, "region order must be in [0, catalogue order]");
   if (cat->groups.size() != 1)

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -189,14 +190,111 @@ __global__ void k_cell_neighbours(const double4* cap, const uint2* grange, uint3
   }
 }
 
+// Plate cells: PlateBins::getBinIndicesWithinRadius (PlateBins.h:73-84) for
+// every sightline i, as a per-sightline neighbour list of cell indices:
+// the platelist plates k (ascending id) whose centre passes
+//   |acos(cos_sep(i, k)) - ring| < max_ang,   ring = 1.5 deg,
+// and that hold sightlines of i's group.  cos_sep has the reference's bits
+// (ref_cos_sep, the host trig of both); the device acos may differ from the
+// host libm's in the last bits, so a test within kPlateEdgeMargin of its
+// threshold is settled on the host: pass 0 records it (key i << 32 | k and
+// the cosine), passes 1 and 2 look up the host's decision.
+constexpr double kPlateEdgeMargin = 1e-12;
+constexpr uint32_t kPlateEdgeCap = 65536;
+// edge buffer: [0] count, [1, 1 + cap) sorted keys, [1 + cap, 1 + 2 cap)
+// pass 0: the cosines' bits, passes 1-2: the host's decisions (0 or 1)
+
+// 1 pass, 0 fail, 2 within the margin
+__device__ __forceinline__ int plate_ring(const SkyTrig& si, const double4 pt, double ring, double max_ang,
+                                          double* c_out) {
+  const double c = ref_cos_sep(si, SkyTrig{pt.x, pt.y, pt.z, pt.w});
+  *c_out = c;
+  const double v = fabs(acos(c) - ring) - max_ang;
+  if (isnan(v)) return 0;  // |c| > 1: acos is NaN on the host too, and NaN < max_ang fails
+  if (v < -kPlateEdgeMargin) return 1;
+  if (v > kPlateEdgeMargin) return 0;
+  return 2;
+}
+
+__device__ bool plate_edge_decision(const unsigned long long* edge, unsigned long long key) {
+  const uint32_t n = (uint32_t)min(edge[0], (unsigned long long)kPlateEdgeCap);
+  uint32_t a = 0, b = n;
+  while (a < b) {
+    const uint32_t m = (a + b) >> 1;
+    if (edge[1 + m] < key) a = m + 1; else b = m;
+  }
+  return a < n && edge[1 + a] == key && edge[1 + kPlateEdgeCap + a] != 0;
+}
+
+// One warp per sightline, lanes over the platelist.  pass 0: record the
+// tests within the margin; pass 1: count[i] = neighbour cells; pass 2: write
+// them at out[start[i] ...] in ascending plate order.
+__global__ void k_plate_neighbours(int pass, const double4* trig, const uint32_t* cell_idx, const uint2* grange,
+                                   const int64_t* cells, size_t n_los, const int32_t* plate_ids,
+                                   const double4* plate_trig, uint32_t n_plates, double ring, double max_ang,
+                                   unsigned long long* edge, uint32_t* count, const uint32_t* start,
+                                   uint32_t* out) {
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t i = warp; i < n_los; i += nwarps) {
+    const double4 ti = trig[i];
+    const SkyTrig si{ti.x, ti.y, ti.z, ti.w};
+    const uint32_t ca = cell_idx[i];
+    const uint2 gr = grange[ca];
+    const int64_t gkey = cells[ca] & ~0xFFFFFFFFll;
+    uint32_t n = 0;
+    const uint32_t o = (pass == 2) ? start[i] : 0;
+    for (uint32_t base = 0; base < n_plates; base += 32) {
+      const uint32_t k = base + lane;
+      bool hit = false;
+      uint32_t cell = 0;
+      if (k < n_plates) {
+        double c;
+        int r = plate_ring(si, plate_trig[k], ring, max_ang, &c);
+        const unsigned long long key = ((unsigned long long)i << 32) | k;
+        if (r == 2) {
+          if (pass == 0) {
+            const unsigned long long slot = atomicAdd(&edge[0], 1ull);
+            if (slot < kPlateEdgeCap) {
+              edge[1 + slot] = key;
+              edge[1 + kPlateEdgeCap + slot] = (unsigned long long)__double_as_longlong(c);
+            }
+          }
+          r = (pass != 0 && plate_edge_decision(edge, key)) ? 1 : 0;
+        }
+        if (r == 1 && pass != 0) {
+          // the cell (group of i, plate k), if occupied: binary search in the group's cells
+          const int64_t want = gkey | (int64_t)plate_ids[k];
+          uint32_t a = gr.x, b = gr.y;
+          while (a < b) {
+            const uint32_t m = (a + b) >> 1;
+            if (cells[m] < want) a = m + 1; else b = m;
+          }
+          if (a < gr.y && cells[a] == want) {
+            hit = true;
+            cell = a;
+          }
+        }
+      }
+      const unsigned m = __ballot_sync(kFull, hit);
+      if (pass == 2 && hit) out[o + n + __popc(m & ((1u << lane) - 1u))] = cell;
+      n += __popc(m);
+    }
+    if (pass == 1 && lane == 0) count[i] = n;
+  }
+}
+
 // One warp per primary sightline (in cell order).  Pass 1 (items == null)
 // counts accepted pairs and candidates; pass 2 writes the accepted pairs at
 // their offsets in a fixed order (neighbour cells ascending, j ascending).
+// The neighbour cells are the CSR nb_start/nb of the primary's cell, or of
+// the primary itself (nb_by_sightline: plate cells).
 // Mirrors skybin_xi_task's loop (XiEstimator.cc:130-152): skip j <= i, cut
 // cos(theta) <= cos_max.
 __global__ void k_expand(const uint32_t* members, uint32_t n_members, const uint32_t* cell_idx,
                          const uint32_t* cell_start, const uint32_t* nb_start, const uint32_t* nb,
-                         const double4* trig, const uint32_t* npix, double cos_max,
+                         int nb_by_sightline, const double4* trig, const uint32_t* npix, double cos_max,
                          uint32_t* cnt, unsigned long long* cand, unsigned long long* cell_pairs,
                          const uint32_t* item_off, uint32_t* item_i, uint32_t* item_j,
                          double* item_c, uint32_t* item_sep, int coord, double theta_min,
@@ -212,7 +310,8 @@ __global__ void k_expand(const uint32_t* members, uint32_t n_members, const uint
     uint32_t n_acc = 0;
     unsigned long long n_cand = 0, n_pairs = 0;
     uint32_t o = item_i ? item_off[p] : 0;
-    for (uint32_t q = nb_start[ca]; q < nb_start[ca + 1]; ++q) {
+    const uint32_t nbk = nb_by_sightline ? i : ca;  // plate cells: sightline i's own list
+    for (uint32_t q = nb_start[nbk]; q < nb_start[nbk + 1]; ++q) {
       const uint32_t cb = nb[q];
       const uint32_t b0 = cell_start[cb], b1 = cell_start[cb + 1];
       for (uint32_t base = b0; base < b1; base += 32) {
@@ -728,7 +827,7 @@ void tos_engine_destroy(tos_engine* e) {
 tos_status tos_catalog_create(tos_engine* e, const tos_sightline* los, size_t n_los,
                               const tos_pixel* pixels, size_t n_pixels, int order,
                               tos_catalog** out) {
-  return tos::catalog_create_impl(e, los, n_los, pixels, n_pixels, order, 0.0, out);
+  return tos::catalog_create_impl(e, los, n_los, pixels, n_pixels, order, 0.0, nullptr, 0, out);
 }
 
 tos_status tos_catalog_create_dc(tos_engine* e, const tos_sightline* los, size_t n_los,
@@ -736,21 +835,34 @@ tos_status tos_catalog_create_dc(tos_engine* e, const tos_sightline* los, size_t
                                  tos_catalog** out) {
   if (!(omega_matter > 0 && omega_matter <= 1))
     return fail(TOS_ERR_INVALID_ARG, "omega_matter must be in (0, 1]");
-  return tos::catalog_create_impl(e, los, n_los, pixels, n_pixels, order, omega_matter, out);
+  return tos::catalog_create_impl(e, los, n_los, pixels, n_pixels, order, omega_matter, nullptr, 0, out);
+}
+
+tos_status tos_catalog_create_plates(tos_engine* e, const tos_sightline* los, size_t n_los,
+                                     const tos_pixel* pixels, size_t n_pixels, const tos_plate* platelist,
+                                     size_t n_plates, double omega_matter, tos_catalog** out) {
+  if (!(omega_matter == 0 || (omega_matter > 0 && omega_matter <= 1)))
+    return fail(TOS_ERR_INVALID_ARG, "omega_matter must be 0 (keep the pixels' distances) or in (0, 1]");
+  if (n_plates > 0 && !platelist) return fail(TOS_ERR_INVALID_ARG, "platelist is null");
+  static const tos_plate kNone{};
+  return tos::catalog_create_impl(e, los, n_los, pixels, n_pixels, 0, omega_matter,
+                                  n_plates ? platelist : &kNone, n_plates, out);
 }
 
 }  // extern "C"
 
 // Catalogue creation; omega_matter > 0: each pixel's distance is computed on
-// the device from its loglam (the pixels' own distances are ignored).
+// the device from its loglam (the pixels' own distances are ignored);
+// platelist != null: the cells are the sightlines' plates.
 tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, size_t n_los,
                                     const tos_pixel* pixels, size_t n_pixels, int order, double omega_matter,
-                                    tos_catalog** out) {
+                                    const tos_plate* platelist, size_t n_plates, tos_catalog** out) {
   if (!e || !out) return fail(TOS_ERR_INVALID_ARG, "engine/out is null");
   *out = nullptr;
   if (n_los == 0 || !los) return fail(TOS_ERR_INVALID_ARG, "no sightlines");
   if (n_los >= 0xFFFFFFF0ull) return fail(TOS_ERR_UNSUPPORTED, "too many sightlines");
-  if (order < 0 || order > 13) return fail(TOS_ERR_INVALID_ARG, "healpix order must be in [0, 13]");
+  const bool plates = platelist != nullptr;
+  if (!plates && (order < 0 || order > 13)) return fail(TOS_ERR_INVALID_ARG, "healpix order must be in [0, 13]");
   if (n_pixels > 0 && !pixels) return fail(TOS_ERR_INVALID_ARG, "pixels is null");
   std::lock_guard<std::mutex> lock(e->mu);
   DeviceGuard g(e->device);
@@ -758,8 +870,14 @@ tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, siz
   cat->eng = e;
   cat->device = e->device;
   cat->n_los = n_los;
-  cat->order = order;
-  cat->nside = (int64_t)1 << order;
+  cat->plates = plates;
+  cat->order = plates ? -1 : order;
+  cat->nside = plates ? 0 : (int64_t)1 << order;
+  // a HEALPix cell's solid angle, or a plate's (radius 1.5 degrees)
+  {
+    const double pi = 3.14159265358979323846, rp = 1.5 * pi / 180.0;
+    cat->cell_sr = plates ? pi * rp * rp : 4.0 * pi / (12.0 * (double)cat->nside * (double)cat->nside);
+  }
   // --- host index: pixel ranges, trig, cells
   cat->npix.resize(n_los);
   cat->off.resize(n_los);
@@ -771,6 +889,8 @@ tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, siz
       return fail(TOS_ERR_INVALID_ARG, "sightline " + std::to_string(s) + " pixel range out of bounds");
     if (!std::isfinite(l.ra) || !std::isfinite(l.dec))
       return fail(TOS_ERR_INVALID_ARG, "sightline " + std::to_string(s) + " has non-finite position");
+    if (plates && l.plate < 0)
+      return fail(TOS_ERR_INVALID_ARG, "sightline " + std::to_string(s) + " has a negative plate id");
     cat->npix[s] = l.num_pixels;
     cat->off[s] = total;
     if (l.pixel_offset != total) contiguous = false;
@@ -786,7 +906,24 @@ tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, siz
                            std::cos(los[s].ra));
     // cells of different groups never meet: the group is the key's high word
     cat->cell_of[s] = ((int64_t)los[s].group << 32) |
-                      healpix_radec2pix(cat->nside, los[s].ra, los[s].dec);
+                      (plates ? (int64_t)los[s].plate : healpix_radec2pix(cat->nside, los[s].ra, los[s].dec));
+  }
+  if (plates) {
+    // PlateBins' platelist (PlateBins.h:38-45): a std::map from plate id to
+    // the centre, ra/dec in degrees times deg2rad (constants.h:12-13)
+    const double deg2rad = (std::atan(1.0) * 4) / 180.0;
+    std::map<int32_t, std::pair<double, double>> list;
+    for (size_t k = 0; k < n_plates; ++k) {
+      if (!std::isfinite(platelist[k].ra_center) || !std::isfinite(platelist[k].dec_center))
+        return fail(TOS_ERR_INVALID_ARG, "platelist row " + std::to_string(k) + " has a non-finite centre");
+      list[platelist[k].plate] = {platelist[k].ra_center * deg2rad, platelist[k].dec_center * deg2rad};
+    }
+    for (const auto& p : list) {
+      cat->plate_ids.push_back(p.first);
+      // SkyObject's cached sines and cosines (types.h:20-26)
+      cat->plate_trig.push_back(make_double4(std::sin(p.second.second), std::cos(p.second.second),
+                                             std::sin(p.second.first), std::cos(p.second.first)));
+    }
   }
   cat->cells = cat->cell_of;
   std::sort(cat->cells.begin(), cat->cells.end());
@@ -851,6 +988,11 @@ tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, siz
   // --- device buffers
   TOS_TRY(cat->d_trig.alloc(n_los));
   TOS_TRY(cat->d_cap.alloc(nc));
+  TOS_TRY(cat->d_cells.alloc(nc));
+  if (plates && !cat->plate_ids.empty()) {
+    TOS_TRY(cat->d_plate_ids.alloc(cat->plate_ids.size()));
+    TOS_TRY(cat->d_plate_trig.alloc(cat->plate_ids.size()));
+  }
   TOS_TRY(cat->d_cell_grange.alloc(nc));
   TOS_TRY(cat->d_group_cell_start.alloc(cat->group_cell_start.size()));
   TOS_TRY(cat->d_cell_idx.alloc(n_los));
@@ -874,6 +1016,14 @@ tos_status tos::catalog_create_impl(tos_engine* e, const tos_sightline* los, siz
                                cudaMemcpyHostToDevice, st));
   TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cap.p, caps.data(), nc * sizeof(double4),
                                cudaMemcpyHostToDevice, st));
+  TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cells.p, cat->cells.data(), nc * sizeof(int64_t),
+                               cudaMemcpyHostToDevice, st));
+  if (!cat->plate_ids.empty()) {
+    TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_plate_ids.p, cat->plate_ids.data(), cat->plate_ids.size() * 4,
+                                 cudaMemcpyHostToDevice, st));
+    TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_plate_trig.p, cat->plate_trig.data(),
+                                 cat->plate_trig.size() * sizeof(double4), cudaMemcpyHostToDevice, st));
+  }
   TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_cell_grange.p, grange.data(), nc * sizeof(uint2),
                                cudaMemcpyHostToDevice, st));
   TOS_CUDA_TRY(cudaMemcpyAsync(cat->d_group_cell_start.p, cat->group_cell_start.data(),
@@ -1054,7 +1204,8 @@ void tos_xibin_finalize(tos_xibin* b, size_t n) {
 namespace tos {
 
 uint64_t catalog_data_bytes(const tos_catalog* c) {
-  uint64_t b = c->d_trig.bytes() + c->d_cap.bytes() + c->d_cell_grange.bytes() +
+  uint64_t b = c->d_trig.bytes() + c->d_cap.bytes() + c->d_cells.bytes() + c->d_plate_ids.bytes() +
+               c->d_plate_trig.bytes() + c->d_cell_grange.bytes() +
                c->d_group_cell_start.bytes() + c->d_cell_idx.bytes() + c->d_cell_start.bytes() +
                c->d_members.bytes() + c->d_npix.bytes() + c->d_off.bytes() + c->d_raw.bytes() +
                c->d_dist_pad.bytes() + c->d_loglam_pad.bytes() + c->d_pack.bytes() + c->d_wd.bytes() +
@@ -1065,7 +1216,8 @@ uint64_t catalog_data_bytes(const tos_catalog* c) {
 }
 
 size_t Workspace::bytes() const {
-  return d_nb_count.bytes() + d_nb_start.bytes() + d_nb.bytes() + d_cnt.bytes() + d_cand.bytes() +
+  return d_nb_count.bytes() + d_nb_start.bytes() + d_nb.bytes() + d_plate_edge.bytes() + d_cnt.bytes() +
+         d_cand.bytes() +
          d_item_off.bytes() + d_item_i.bytes() + d_item_j.bytes() + d_item_sep.bytes() +
          d_item_c.bytes() + d_cell_pairs.bytes() + d_acc.bytes() + d_out.bytes() +
          d_counters.bytes() + d_thr.bytes() + d_gq.bytes() + d_cub_tmp.bytes();
@@ -1140,10 +1292,67 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
   const double cos_max = std::cos(max_ang);  // XiEstimator.cc:25
 
   // --- cell neighbours
-  TOS_TRY(ws->d_nb_count.alloc(nc));
-  TOS_TRY(ws->d_nb_start.alloc(nc + 1));
   TOS_CUDA_TRY(cudaEventRecord(e->ev[0], st));
-  {
+  if (cat->plates) {
+    // per sightline: the occupied plates of PlateBins' ring test
+    const size_t nl = cat->n_los;
+    const uint32_t np = (uint32_t)cat->plate_ids.size();
+    const double ring = 1.5 * ((std::atan(1.0) * 4) / 180.0);  // 1.5*deg2rad, PlateBins.h:80
+    TOS_TRY(ws->d_nb_count.alloc(nl));
+    TOS_TRY(ws->d_nb_start.alloc(nl + 1));
+    TOS_TRY(ws->d_plate_edge.alloc(1 + 2 * (size_t)kPlateEdgeCap));
+    unsigned long long* edge = ws->d_plate_edge.p;
+    TOS_CUDA_TRY(cudaMemsetAsync(edge, 0, sizeof(unsigned long long), st));
+    TOS_CUDA_TRY(cudaMemsetAsync(ws->d_nb_count.p, 0, nl * 4, st));
+    const int gp = grid_for(e, nl * 32, 256);
+    if (np > 0) {
+      k_plate_neighbours<<<gp, 256, 0, st>>>(0, cat->d_trig.p, cat->d_cell_idx.p, cat->d_cell_grange.p,
+                                             cat->d_cells.p, nl, cat->d_plate_ids.p, cat->d_plate_trig.p, np,
+                                             ring, max_ang, edge, nullptr, nullptr, nullptr);
+      TOS_CUDA_TRY(cudaGetLastError());
+      unsigned long long ne = 0;
+      TOS_CUDA_TRY(cudaMemcpyAsync(&ne, edge, 8, cudaMemcpyDeviceToHost, st));
+      TOS_CUDA_TRY(cudaStreamSynchronize(st));
+      if (ne > kPlateEdgeCap)
+        return fail(TOS_ERR_UNSUPPORTED, std::to_string(ne) + " sightline-plate angles lie within 1e-12 rad of "
+                                         "the plate ring's edge (at most 65536 are settled on the host)");
+      if (ne) {
+        // settled with the host libm's acos, the function PlateBins calls
+        std::vector<unsigned long long> keys(ne), cbits(ne), sk(ne), dec(ne);
+        TOS_CUDA_TRY(cudaMemcpy(keys.data(), edge + 1, ne * 8, cudaMemcpyDeviceToHost));
+        TOS_CUDA_TRY(cudaMemcpy(cbits.data(), edge + 1 + kPlateEdgeCap, ne * 8, cudaMemcpyDeviceToHost));
+        std::vector<size_t> ord(ne);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return keys[a] < keys[b]; });
+        for (size_t t = 0; t < ne; ++t) {
+          double c;
+          std::memcpy(&c, &cbits[ord[t]], 8);
+          sk[t] = keys[ord[t]];
+          dec[t] = (std::fabs(std::acos(c) - ring) < max_ang) ? 1ull : 0ull;
+        }
+        TOS_CUDA_TRY(cudaMemcpy(edge + 1, sk.data(), ne * 8, cudaMemcpyHostToDevice));
+        TOS_CUDA_TRY(cudaMemcpy(edge + 1 + kPlateEdgeCap, dec.data(), ne * 8, cudaMemcpyHostToDevice));
+      }
+      k_plate_neighbours<<<gp, 256, 0, st>>>(1, cat->d_trig.p, cat->d_cell_idx.p, cat->d_cell_grange.p,
+                                             cat->d_cells.p, nl, cat->d_plate_ids.p, cat->d_plate_trig.p, np,
+                                             ring, max_ang, edge, ws->d_nb_count.p, nullptr, nullptr);
+      TOS_CUDA_TRY(cudaGetLastError());
+    }
+    std::vector<uint32_t> nbc(nl), nbs(nl + 1, 0);
+    TOS_CUDA_TRY(cudaMemcpyAsync(nbc.data(), ws->d_nb_count.p, nl * 4, cudaMemcpyDeviceToHost, st));
+    TOS_CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < nl; ++i) nbs[i + 1] = nbs[i] + nbc[i];
+    TOS_TRY(ws->d_nb.alloc(nbs[nl]));
+    TOS_CUDA_TRY(cudaMemcpyAsync(ws->d_nb_start.p, nbs.data(), (nl + 1) * 4, cudaMemcpyHostToDevice, st));
+    if (np > 0 && nbs[nl] > 0) {
+      k_plate_neighbours<<<gp, 256, 0, st>>>(2, cat->d_trig.p, cat->d_cell_idx.p, cat->d_cell_grange.p,
+                                             cat->d_cells.p, nl, cat->d_plate_ids.p, cat->d_plate_trig.p, np,
+                                             ring, max_ang, edge, nullptr, ws->d_nb_start.p, ws->d_nb.p);
+      TOS_CUDA_TRY(cudaGetLastError());
+    }
+  } else {
+    TOS_TRY(ws->d_nb_count.alloc(nc));
+    TOS_TRY(ws->d_nb_start.alloc(nc + 1));
     const int gb = grid_for(e, nc, 128);
     k_cell_neighbours<<<gb, 128, 0, st>>>(cat->d_cap.p, cat->d_cell_grange.p, nc, max_ang,
                                           nullptr, ws->d_nb_count.p, nullptr);
@@ -1176,7 +1385,7 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
   const double theta_min = G.axis[1].min, theta_inv = 1.0 / axis_width(G.axis[1]);
   const int ge = grid_for(e, (size_t)nm * 32, 256);
   k_expand<<<ge, 256, 0, st>>>(cat->d_members.p, nm, cat->d_cell_idx.p, cat->d_cell_start.p,
-                               ws->d_nb_start.p, ws->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
+                               ws->d_nb_start.p, ws->d_nb.p, cat->plates ? 1 : 0, cat->d_trig.p, cat->d_npix.p, cos_max,
                                ws->d_cnt.p, ws->d_cand.p, ws->d_cell_pairs.p, nullptr, nullptr,
                                nullptr, nullptr, nullptr, G.type, theta_min, theta_inv, ctr + 16);
   TOS_CUDA_TRY(cudaGetLastError());
@@ -1237,7 +1446,7 @@ tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos
   TOS_TRY(ws->d_item_c.alloc(n_items));
   TOS_TRY(ws->d_item_sep.alloc(G.type == TOS_OBSERVING ? n_items : 1));
   k_expand<<<ge, 256, 0, st>>>(cat->d_members.p, nm, cat->d_cell_idx.p, cat->d_cell_start.p,
-                               ws->d_nb_start.p, ws->d_nb.p, cat->d_trig.p, cat->d_npix.p, cos_max,
+                               ws->d_nb_start.p, ws->d_nb.p, cat->plates ? 1 : 0, cat->d_trig.p, cat->d_npix.p, cos_max,
                                ws->d_cnt.p, ws->d_cand.p, ws->d_cell_pairs.p, ws->d_item_off.p,
                                ws->d_item_i.p, ws->d_item_j.p, ws->d_item_c.p,
                                ws->d_item_sep.p, G.type, theta_min, theta_inv, ctr + 16);

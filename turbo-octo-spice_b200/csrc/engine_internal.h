@@ -70,7 +70,8 @@ namespace tos {
 // runs again (a server slot, the catalogue's own runs) allocates only when a
 // run needs more than before.
 struct Workspace {
-  DevBuf<uint32_t> d_nb_count, d_nb_start, d_nb;  // cell neighbour CSR
+  DevBuf<uint32_t> d_nb_count, d_nb_start, d_nb;  // cell neighbour CSR (per sightline for plate cells)
+  DevBuf<unsigned long long> d_plate_edge;        // plate-ring tests within the margin (plate cells)
   DevBuf<uint32_t> d_cnt;                         // per primary: accepted pairs
   DevBuf<unsigned long long> d_cand;              // per primary candidates (for stats)
   DevBuf<uint32_t> d_item_off;
@@ -113,10 +114,19 @@ struct tos_catalog {
   tos_engine* eng = nullptr;
   int device = 0;
   size_t n_los = 0, n_pix = 0;
-  int order = 0;
+  int order = 0;                    // HEALPix order (-1: plate cells)
   int64_t nside = 0;
+  double cell_sr = 0;               // solid angle of a cell (work estimates)
+  // plate cells (tos_catalog_create_plates): the platelist's plates in
+  // ascending id (a repeated id: its last row) and their centres
+  bool plates = false;
+  std::vector<int32_t> plate_ids;
+  std::vector<double4> plate_trig;  // sin_dec, cos_dec, sin_ra, cos_ra of the centre
+  tos::DevBuf<int32_t> d_plate_ids;
+  tos::DevBuf<double4> d_plate_trig;
+  tos::DevBuf<int64_t> d_cells;     // `cells` on the device (plate-cell lookup)
   // host-side index
-  std::vector<int64_t> cell_of;     // cell id of each sightline: group << 32 | HEALPix pixel
+  std::vector<int64_t> cell_of;     // cell id of each sightline: group << 32 | HEALPix pixel (or plate)
   std::vector<int64_t> cells;       // occupied cells, ascending
   std::vector<double4> caps;        // per cell: unit centre xyz and angular radius of its members
   std::vector<uint32_t> groups;     // distinct sightline groups, ascending
@@ -183,16 +193,14 @@ struct RowPlan {
   std::function<uint64_t(const std::vector<uint64_t>& cell_items)> max_row_items;
 };
 
-// The pair count behind tos_xi_run, with its scratch in `ws` (the caller
-// owns ws exclusively for the call): plan = null accumulates per cell (and
-// honours TOS_XI_SUBSAMPLES / TOS_XI_PER_GROUP), otherwise into the plan's
-// slots, combined by plan->combine.  Takes the engine lock; the catalogue is
-// only read, so runs with different workspaces may share it.
-// Catalogue creation behind tos_catalog_create and tos_catalog_create_dc;
-// omega_matter > 0: each pixel's distance is computed on the device from its
-// loglam (the pixels' own distances are ignored).
+// Catalogue creation behind tos_catalog_create, tos_catalog_create_dc and
+// tos_catalog_create_plates; omega_matter > 0: each pixel's distance is
+// computed on the device from its loglam (the pixels' own distances are
+// ignored).  platelist != null: cells are the sightlines' plates (order is
+// not used).
 tos_status catalog_create_impl(tos_engine* e, const tos_sightline* los, size_t n_los, const tos_pixel* pixels,
-                               size_t n_pixels, int order, double omega_matter, tos_catalog** out);
+                               size_t n_pixels, int order, double omega_matter, const tos_plate* platelist,
+                               size_t n_plates, tos_catalog** out);
 
 // How a run shares the GPU with runs on other streams (the request
 // server): the dominant kernel (grid or diagonal sweep) is launched in
@@ -209,6 +217,11 @@ struct SweepShare {
   int chunks = 16;  // chunks per run (fewer when a run has few sightline pairs)
 };
 
+// The pair count behind tos_xi_run, with its scratch in `ws` (the caller
+// owns ws exclusively for the call): plan = null accumulates per cell (and
+// honours TOS_XI_SUBSAMPLES / TOS_XI_PER_GROUP), otherwise into the plan's
+// slots, combined by plan->combine.  Takes the engine lock; the catalogue is
+// only read, so runs with different workspaces may share it.
 tos_status xi_run_impl(tos_engine* e, tos_catalog* cat, Workspace* ws, const tos_grid* grid,
                        double scale, uint32_t flags, const RowPlan* plan, tos_xibin* out_bins,
                        tos_xibin* out_cells, tos_xi_stats* stats, const SweepShare* share = nullptr);

@@ -140,6 +140,8 @@ extern "C" tos_status tos_xi_run_jackknife(tos_engine* e, tos_catalog* cat, cons
   if (cat->device != e->device) return fail(TOS_ERR_INVALID_ARG, "catalogue is on another device");
   if (flags & ~TOS_XI_EXACT)
     return fail(TOS_ERR_INVALID_ARG, "a jackknife run takes no flag but TOS_XI_EXACT");
+  if (cat->plates)
+    return fail(TOS_ERR_UNSUPPORTED, "jackknife regions are HEALPix pixels: a plate catalogue has none");
   if (region_order < 0 || region_order > cat->order)
     return fail(TOS_ERR_INVALID_ARG, "region order must be in [0, catalogue order]");
   double max_ang = 0;

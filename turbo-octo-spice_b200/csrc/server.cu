@@ -64,7 +64,7 @@ constexpr double kPi = 3.14159265358979323846;
 // cells, with a 1.5 margin).
 double pairs_estimate(const tos_catalog* cat, const tos_grid& g, double scale) {
   const double nc = (double)cat->cells.size(), n = (double)cat->n_los;
-  const double cell_sr = 4.0 * kPi / (12.0 * (double)cat->nside * (double)cat->nside);
+  const double cell_sr = cat->cell_sr;
   const double area = std::max(nc * cell_sr, cell_sr);
   const double ang = std::min(max_angular_scale(g, scale), kPi);
   const double disc = 2.0 * kPi * (1.0 - std::cos(ang));
@@ -74,7 +74,7 @@ double pairs_estimate(const tos_catalog* cat, const tos_grid& g, double scale) {
 uint64_t workspace_estimate(const tos_catalog* cat, const tos_grid& g, double scale, size_t n_rows) {
   const double nb = (double)g.axis[0].nbins * g.axis[1].nbins * g.axis[2].nbins;
   const double nc = (double)cat->cells.size(), n = (double)cat->n_los;
-  const double cell_sr = 4.0 * kPi / (12.0 * (double)cat->nside * (double)cat->nside);
+  const double cell_sr = cat->cell_sr;
   const double area = std::max(nc * cell_sr, cell_sr);
   const double ang = std::min(max_angular_scale(g, scale), kPi);
   const double disc = 2.0 * kPi * (1.0 - std::cos(ang));

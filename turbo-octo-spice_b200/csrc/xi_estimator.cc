@@ -85,8 +85,20 @@ double TwoPointGrid::maxAngularScale(double scale) const {
 XiEstimator::XiEstimator(double scale, const TwoPointGrid& grid, BinningCoordinateType type,
                          const std::vector<Forest>& sightlines, int healpix_order, int device)
     : scale_(scale), grid_(grid) {
+  build(type, sightlines, healpix_order, nullptr, device);
+}
+
+XiEstimator::XiEstimator(double scale, const TwoPointGrid& grid, BinningCoordinateType type,
+                         const std::vector<Forest>& sightlines, const std::vector<tos_plate>& platelist,
+                         int device)
+    : scale_(scale), grid_(grid) {
+  build(type, sightlines, 0, &platelist, device);
+}
+
+void XiEstimator::build(BinningCoordinateType type, const std::vector<Forest>& sightlines, int healpix_order,
+                        const std::vector<tos_plate>* platelist, int device) {
   static const tos_coord_type map[3] = {TOS_POLAR, TOS_CARTESIAN, TOS_OBSERVING};
-  if ((int)type < 0 || (int)type > 2 || map[type] != (tos_coord_type)grid.desc().type)
+  if ((int)type < 0 || (int)type > 2 || map[type] != (tos_coord_type)grid_.desc().type)
     throw RuntimeError("coordinate type does not match the grid");
   std::vector<tos_sightline> los(sightlines.size());
   std::vector<tos_pixel> px;
@@ -107,7 +119,9 @@ XiEstimator::XiEstimator(double scale, const TwoPointGrid& grid, BinningCoordina
   num_sightlines_ = sightlines.size();
   check(tos_engine_create(device, &engine_));
   const tos_status s =
-      tos_catalog_create(engine_, los.data(), los.size(), px.data(), px.size(), healpix_order, &catalog_);
+      platelist ? tos_catalog_create_plates(engine_, los.data(), los.size(), px.data(), px.size(),
+                                            platelist->data(), platelist->size(), 0.0, &catalog_)
+                : tos_catalog_create(engine_, los.data(), los.size(), px.data(), px.size(), healpix_order, &catalog_);
   if (s != TOS_OK) {
     tos_engine_destroy(engine_);
     engine_ = nullptr;

@@ -60,6 +60,10 @@ class XiEstimator {
   // the HealpixBins order (nside = 2^order); device: CUDA device id.
   XiEstimator(double scale, const TwoPointGrid& grid, BinningCoordinateType type,
               const std::vector<Forest>& sightlines, int healpix_order, int device = 0);
+  // The same with the sightlines binned by plate (PlateBins, PlateBins.h:18-92):
+  // platelist holds the PLATE, RACEN, DECCEN rows of the platelist file.
+  XiEstimator(double scale, const TwoPointGrid& grid, BinningCoordinateType type,
+              const std::vector<Forest>& sightlines, const std::vector<tos_plate>& platelist, int device = 0);
   ~XiEstimator();
   XiEstimator(const XiEstimator&) = delete;
   XiEstimator& operator=(const XiEstimator&) = delete;
@@ -78,6 +82,8 @@ class XiEstimator {
   const std::vector<double>& covariance() const { return cov_; }
 
  private:
+  void build(BinningCoordinateType type, const std::vector<Forest>& sightlines, int healpix_order,
+             const std::vector<tos_plate>* platelist, int device);
   double scale_;
   TwoPointGrid grid_;
   tos_engine* engine_ = nullptr;

@@ -32,6 +32,8 @@ SIGHTLINE_DTYPE = np.dtype([("ra", "<f8"), ("dec", "<f8"), ("forest_id", "<i4"),
                             ("pixel_offset", "<u8"), ("num_pixels", "<u4"), ("group", "<u4")])
 XIBIN_DTYPE = np.dtype([("didj", "<f8"), ("di", "<f8"), ("dj", "<f8"), ("wgt", "<f8"), ("wi", "<f8"),
                         ("wj", "<f8"), ("z", "<f8"), ("num_pairs", "<i8")])
+# one platelist row: PLATE, RACEN, DECCEN (degrees), the columns PlateBins reads
+PLATE_DTYPE = np.dtype([("plate", "<i4"), ("ra_center", "<f4"), ("dec_center", "<f4")])
 
 
 class TosError(RuntimeError):
@@ -132,6 +134,7 @@ def lib() -> C.CDLL:
         L.tos_fill_distances.argtypes = [dbl, vp, sz]
         L.tos_catalog_create_dc.argtypes = [vp, vp, sz, vp, sz, i32, dbl, C.POINTER(vp)]
         L.tos_catalog_distances.argtypes = [vp, vp, sz]
+        L.tos_catalog_create_plates.argtypes = [vp, vp, sz, vp, sz, vp, sz, dbl, C.POINTER(vp)]
         for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
                      "tos_catalog_sightline_cells", "tos_grid_max_angular_scale", "tos_xi_run",
                      "tos_brute_run", "tos_brute_tune", "tos_comoving_distance", "tos_fill_distances"):
@@ -245,17 +248,31 @@ class Engine:
 
 
 class Catalog:
-    """Sightlines and pixels resident on the device, binned into HEALPix cells."""
+    """Sightlines and pixels resident on the device, binned into HEALPix cells
+    (HealpixBins) or, with a platelist, into their plates (PlateBins)."""
 
-    def __init__(self, engine: Engine, sightlines: np.ndarray, pixels: np.ndarray, healpix_order: int,
-                 omega_matter: float = None):
+    def __init__(self, engine: Engine, sightlines: np.ndarray, pixels: np.ndarray, healpix_order: int = None,
+                 omega_matter: float = None, platelist: np.ndarray = None):
         """With omega_matter, each pixel's comoving distance is computed on the
         device from its loglam (tos_catalog_create_dc; the pixels' own
-        distances are ignored), with the same bits as fill_distances."""
+        distances are ignored), with the same bits as fill_distances.  With
+        platelist (PLATE_DTYPE rows: PLATE, RACEN, DECCEN in degrees) the
+        cells are the sightlines' `plate` ids (tos_catalog_create_plates) and
+        healpix_order must be None."""
         sightlines = np.ascontiguousarray(sightlines, dtype=SIGHTLINE_DTYPE)
         pixels = np.ascontiguousarray(pixels, dtype=PIXEL_DTYPE)
         h = C.c_void_p()
-        if omega_matter is None:
+        if platelist is not None:
+            if healpix_order is not None:
+                raise ValueError("a plate catalogue takes no HEALPix order")
+            plates = np.ascontiguousarray(platelist, dtype=PLATE_DTYPE)
+            _check(lib().tos_catalog_create_plates(engine.handle, _ptr(sightlines), len(sightlines), _ptr(pixels),
+                                                   len(pixels), _ptr(plates) if len(plates) else None, len(plates),
+                                                   0.0 if omega_matter is None else float(omega_matter),
+                                                   C.byref(h)))
+        elif healpix_order is None:
+            raise ValueError("healpix_order is needed without a platelist")
+        elif omega_matter is None:
             _check(lib().tos_catalog_create(engine.handle, _ptr(sightlines), len(sightlines), _ptr(pixels),
                                             len(pixels), healpix_order, C.byref(h)))
         else:

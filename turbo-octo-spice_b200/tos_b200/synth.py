@@ -24,7 +24,7 @@ import math
 
 import numpy as np
 
-from . import PIXEL_DTYPE, SIGHTLINE_DTYPE
+from . import PIXEL_DTYPE, PLATE_DTYPE, SIGHTLINE_DTYPE
 
 LYA = 1216.0
 LOG_LYA = math.log10(LYA)
@@ -115,6 +115,36 @@ def small_patch(n: int = 2000, seed: int = 1, ra0_deg: float = 180.0, dec0_deg: 
     s0, s1 = math.sin(math.radians(dec0_deg)), math.sin(math.radians(dec0_deg + size_deg))
     dec = np.arcsin(rng.uniform(s0, s1, n))
     return forest_catalog(ra, dec, seed + 1000, **kw)
+
+
+def plate_tiling(sightlines: np.ndarray, spacing_deg: float = 2.0, first_plate: int = 3000):
+    """BOSS-like plates over a catalogue: centres on a lattice of the given
+    spacing (in dec, and in ra scaled by 1/cos dec) covering the sightlines,
+    each sightline on the plate of the nearest centre (a BOSS plate's fibres
+    lie within 1.49 degrees of its centre).  Returns (sightlines with their
+    `plate` set, the platelist as PLATE_DTYPE rows of every lattice plate,
+    ids first_plate, first_plate + 1, ...; plates may hold no sightline)."""
+    ra = np.degrees(np.asarray(sightlines["ra"], dtype=np.float64))
+    dec = np.degrees(np.asarray(sightlines["dec"], dtype=np.float64))
+    d0, d1 = dec.min() - spacing_deg, dec.max() + spacing_deg
+    cra, cdec = [], []
+    for dc in np.arange(d0, d1 + 1e-9, spacing_deg):
+        step = spacing_deg / max(math.cos(math.radians(dc)), 0.05)
+        for rc in np.arange(ra.min() - step, ra.max() + step + 1e-9, step):
+            cra.append(rc % 360.0)
+            cdec.append(dc)
+    plates = np.zeros(len(cra), dtype=PLATE_DTYPE)
+    plates["plate"] = first_plate + np.arange(len(cra))
+    plates["ra_center"] = np.asarray(cra, dtype=np.float32)
+    plates["dec_center"] = np.asarray(cdec, dtype=np.float32)
+    # nearest centre on the sphere
+    u = np.stack([np.cos(np.radians(dec)) * np.cos(np.radians(ra)), np.cos(np.radians(dec)) * np.sin(np.radians(ra)),
+                  np.sin(np.radians(dec))], 1)
+    pr, pd = np.radians(plates["ra_center"].astype(np.float64)), np.radians(plates["dec_center"].astype(np.float64))
+    v = np.stack([np.cos(pd) * np.cos(pr), np.cos(pd) * np.sin(pr), np.sin(pd)], 1)
+    out = np.array(sightlines, copy=True)
+    out["plate"] = plates["plate"][np.argmax(u @ v.T, axis=1)]
+    return out, plates
 
 
 def _healpix_centres_nside8():
