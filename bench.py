@@ -434,24 +434,29 @@ def engine_arm(args, D):
         D.barrier()
         clk = ClockSampler(dev)
         clk.start()
-        ms_dev = ms_pairs = ms_grid = 0.0
+        ms_dev = ms_pairs = ms_grid = ms_diag = 0.0
         for _ in range(args.steps):
             bins, _, st = T.xi_run(eng, cat, W["grid"], W["scale"])
             ms_dev += st["ms_device"]
             ms_pairs += st["ms_pairs"]
             ms_grid += st["ms_grid"]
+            ms_diag += st["ms_diag"]
         clocks = clk.stop()
         torch.cuda.synchronize(dev)
         D.barrier()
         pairs = int(st["num_pixel_pairs"])
         ms_max = D.max(ms_dev)
         value = D.world * pairs * args.steps / (ms_max / 1e3)
-        # dominant kernel: the grid sweep when it took (nearly) every sightline pair
-        grid_frac = st["num_grid_items"] / max(1, st["num_sightline_pairs_used"])
-        by_grid = grid_frac >= 0.99
-        kernel_ms = (ms_grid if by_grid else ms_pairs) / args.steps
-        kernel_name = ("grid_kernel" if by_grid else
-                       "pair_kernel" if st["num_run_items"] == 0 else "grid/run/pair kernels")
+        # dominant kernel: the grid sweep (Cartesian) or the diagonal sweep
+        # (Polar) when it took (nearly) every sightline pair
+        used = max(1, st["num_sightline_pairs_used"])
+        if st["num_grid_items"] >= 0.99 * used:
+            kernel_name, kernel_ms = "grid_kernel", ms_grid / args.steps
+        elif st["num_diag_items"] >= 0.99 * used:
+            kernel_name, kernel_ms = "diag_kernel", ms_diag / args.steps
+        else:
+            kernel_name = "pair_kernel" if st["num_run_items"] == 0 else "grid/run/pair kernels"
+            kernel_ms = ms_pairs / args.steps
         evaluated = int(st["num_pixel_pairs_evaluated"])
         launches = LAUNCHES_PER_RUN * args.steps
         jk = par = pol = None
