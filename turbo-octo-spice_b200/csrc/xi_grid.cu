@@ -96,8 +96,11 @@ struct GridAcc {
 // there.  The lane of boundary b owns run t0 + b and reads the run's far end
 // from lane b + 1: when the two codes agree, every column of the run has that
 // code (the code is non-decreasing along a row), so the run is added from the
-// two prefix sums without evaluating anything else; otherwise the far end is
-// evaluated and the run split by bisection.  Each lane sums its run into FP64
+// two prefix sums without evaluating anything else.  When they differ by one
+// code (the common case: a run spans a few columns) the run has one change
+// point, found by bisection between its first column and the neighbour's;
+// otherwise the run's last column is evaluated and the run split by
+// bisection.  Each lane sums its run into FP64
 // registers across the rows (its first-axis bin is fixed; its r_perp code
 // moves slowly from row to row) and adds them to the per-cell sums when its
 // codes move on.
@@ -188,6 +191,23 @@ __device__ __forceinline__ void grid_pass(const PairArgs& A, const SweepItem& it
         add_sums<COORD>(A, d, R, k, 0, be - b, ewd - pwd.x, ew - pwd.y, el - pl, acc);
       } else if (code == ce) {
         if (code >= 0 && code < n1) add_sums<COORD>(A, d, R, k, code, be - b, ewd - pwd.x, ew - pwd.y, el - pl, acc);
+      } else if (ce == code + 1) {
+        // One code step between the run's first column and column hi (be,
+        // or the last column nj - 1 when be = nj: the neighbour's code is
+        // that column's), so exactly one change point p in (b, hi]: the
+        // first column whose code exceeds `code`.  p = be: no change inside.
+        int lo = b + 1, hi = min(be, nj - 1);
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (perp_code<MINPOS>(A, R, colx[mid], c, rech) > code) hi = mid; else lo = mid + 1;
+        }
+        if (lo >= be) {
+          if (code >= 0 && code < n1) add_sums<COORD>(A, d, R, k, code, be - b, ewd - pwd.x, ew - pwd.y, el - pl, acc);
+        } else {
+          const double4 pp = pre[lo];
+          if (code >= 0 && code < n1) add_sums<COORD>(A, d, R, k, code, lo - b, pp.x - pwd.x, pp.y - pwd.y, pp.z - pl, acc);
+          if (ce >= 0 && ce < n1) add_sums<COORD>(A, d, R, k, ce, be - lo, ewd - pp.x, ew - pp.y, el - pp.z, acc);
+        }
       } else {
         do_run_from<COORD, MINPOS>(A, d, colx, pre, c, R, k, b, be, code, acc, rech);
       }
