@@ -130,5 +130,29 @@ __device__ __forceinline__ bool diag_item(const PairArgs& A, double zlo, double 
   return A.diag_split && zlo > -1.0 && zhi < 2147483648.0 && zb_lo == zb_hi;
 }
 
+// The kernel that takes item idx, from the predicates above as each kernel
+// applies them (load_item and grid_item for the sweeps, the pixel-pair
+// kernel's own test): one lane per item, so that a kernel can claim a batch
+// of items and skip the others' without loading each one warp-wide.
+enum ItemOwner { kOwnerNone = 0, kOwnerGrid, kOwnerRun, kOwnerDiag, kOwnerPair };
+__device__ __forceinline__ int item_owner(const PairArgs& A, unsigned long long idx) {
+  const uint32_t i = A.item_i[idx], j = A.item_j[idx];
+  if (A.npix[i] == 0 || A.npix[j] == 0) return kOwnerNone;
+  const float4 ri = A.range[i], rj = A.range[j];
+  const float lsum_lo = __fadd_rn(ri.z, rj.z), lsum_hi = __fadd_rn(ri.w, rj.w);
+  const double zlo = dmul(dsub(dmul(0.5, (double)lsum_lo), A.g.min2), A.g.invn2);
+  const double zhi = dmul(dsub(dmul(0.5, (double)lsum_hi), A.g.min2), A.g.invn2);
+  const uint32_t zb_lo = zbin_of_sum(lsum_lo, A.g), zb_hi = zbin_of_sum(lsum_hi, A.g);
+  const bool zconst = zlo > -1.0 && zhi < 2147483648.0 && zb_lo == zb_hi;
+  if (A.run_split && run_item(A, A.item_c[idx], zconst)) return grid_item(A, i, j) ? kOwnerGrid : kOwnerRun;
+  if (diag_item(A, zlo, zhi, zb_lo, zb_hi)) return kOwnerDiag;
+  return kOwnerPair;
+}
+
+// Items per claim of a kernel that takes few of the items (the run sweep and
+// the pixel-pair kernel beside the grid or diagonal sweep): a warp claims 32
+// with one atomic and keeps its own.
+constexpr int kClaimItems = 32;
+
 }  // namespace
 }  // namespace tos

@@ -488,44 +488,50 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) pair_kernel(PairArgs A) {
   __syncwarp();
   unsigned long long n_eval = 0, n_recheck = 0;
   for (;;) {
-    unsigned long long idx = 0;
-    if (lane == 0) idx = atomicAdd(A.next_item, 1ull);
-    idx = __shfl_sync(kFull, idx, 0);
-    if (idx >= A.n_items) break;
-    Item it;
-    it.i = A.item_i[idx];
-    it.j = A.item_j[idx];
-    it.c = A.item_c[idx];
-    it.ni = A.npix[it.i];
-    it.nj = A.npix[it.j];
-    if (it.ni == 0 || it.nj == 0) continue;
-    it.cell = dest_row(A, it.i, it.j);
-    it.sep = (COORD == kObs) ? A.item_sep[idx] : 0u;
-    const uint64_t oj = A.off[it.j] + (uint64_t)kPad * (it.j + 1);
-    it.cold = A.dist_pad + oj;
-    it.coll = A.loglam_pad + oj;
-    it.colx = (COORD == kObs) ? it.coll : it.cold;
-    it.pre = A.prefix + A.off[it.j] + it.j;
-    const double a = 2.0 * dsub(1.0, it.c);
-    it.ap = (COORD == kCart) ? (float)(a * A.g.inv1 * A.g.inv1) : (float)a;
-    // z index: constant over the item when both ends of the loglam-sum range agree
-    const float4 ri = A.range[it.i], rj = A.range[it.j];
-    const float lsum_lo = __fadd_rn(ri.z, rj.z), lsum_hi = __fadd_rn(ri.w, rj.w);
-    const double zlo = dmul(dsub(dmul(0.5, (double)lsum_lo), A.g.min2), A.g.invn2);
-    const double zhi = dmul(dsub(dmul(0.5, (double)lsum_hi), A.g.min2), A.g.invn2);
-    it.zb = zbin_of_sum(lsum_lo, A.g);
-    const uint32_t zb_hi = zbin_of_sum(lsum_hi, A.g);
-    it.zconst = (zlo > -1.0 && zhi < 2147483648.0 && it.zb == zb_hi) ? 1 : 0;
-    it.lo1 = 0;
-    if (A.run_split && run_item(A, it.c, it.zconst)) continue;  // run-sweep kernel's item
-    if (diag_item(A, zlo, zhi, it.zb, zb_hi)) continue;          // diagonal-sweep kernel's item
-    // with run_split or diag_split every field uses the wide fixed-point
-    // scale, which only the direct (exact) path supports
-    const bool exact_item = A.force_exact || !it.zconst || A.run_split || A.diag_split;
-    if (exact_item)
-      process_item<COORD, EXACT0, MINPOS, 1>(A, it, win, lane, n_eval, n_recheck);
-    else
-      process_item<COORD, EXACT0, MINPOS, 0>(A, it, win, lane, n_eval, n_recheck);
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(A.next_item, (unsigned long long)kClaimItems);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= A.n_items) break;
+    const unsigned long long mine = base + lane;
+    unsigned todo = __ballot_sync(kFull, mine < A.n_items && item_owner(A, mine) == kOwnerPair);
+    while (todo) {
+      const unsigned long long idx = base + (__ffs(todo) - 1);
+      todo &= todo - 1;
+      Item it;
+      it.i = A.item_i[idx];
+      it.j = A.item_j[idx];
+      it.c = A.item_c[idx];
+      it.ni = A.npix[it.i];
+      it.nj = A.npix[it.j];
+      if (it.ni == 0 || it.nj == 0) continue;
+      it.cell = dest_row(A, it.i, it.j);
+      it.sep = (COORD == kObs) ? A.item_sep[idx] : 0u;
+      const uint64_t oj = A.off[it.j] + (uint64_t)kPad * (it.j + 1);
+      it.cold = A.dist_pad + oj;
+      it.coll = A.loglam_pad + oj;
+      it.colx = (COORD == kObs) ? it.coll : it.cold;
+      it.pre = A.prefix + A.off[it.j] + it.j;
+      const double a = 2.0 * dsub(1.0, it.c);
+      it.ap = (COORD == kCart) ? (float)(a * A.g.inv1 * A.g.inv1) : (float)a;
+      // z index: constant over the item when both ends of the loglam-sum range agree
+      const float4 ri = A.range[it.i], rj = A.range[it.j];
+      const float lsum_lo = __fadd_rn(ri.z, rj.z), lsum_hi = __fadd_rn(ri.w, rj.w);
+      const double zlo = dmul(dsub(dmul(0.5, (double)lsum_lo), A.g.min2), A.g.invn2);
+      const double zhi = dmul(dsub(dmul(0.5, (double)lsum_hi), A.g.min2), A.g.invn2);
+      it.zb = zbin_of_sum(lsum_lo, A.g);
+      const uint32_t zb_hi = zbin_of_sum(lsum_hi, A.g);
+      it.zconst = (zlo > -1.0 && zhi < 2147483648.0 && it.zb == zb_hi) ? 1 : 0;
+      it.lo1 = 0;
+      if (A.run_split && run_item(A, it.c, it.zconst)) continue;  // run-sweep kernel's item
+      if (diag_item(A, zlo, zhi, it.zb, zb_hi)) continue;          // diagonal-sweep kernel's item
+      // with run_split or diag_split every field uses the wide fixed-point
+      // scale, which only the direct (exact) path supports
+      const bool exact_item = A.force_exact || !it.zconst || A.run_split || A.diag_split;
+      if (exact_item)
+        process_item<COORD, EXACT0, MINPOS, 1>(A, it, win, lane, n_eval, n_recheck);
+      else
+        process_item<COORD, EXACT0, MINPOS, 0>(A, it, win, lane, n_eval, n_recheck);
+    }
   }
   // counters
 #pragma unroll

@@ -107,16 +107,22 @@ __global__ void __launch_bounds__(kRunWarps * 32, 4) run_kernel(PairArgs args) {
   const int n0 = (int)A.g.n0;
   const float tmax = A.thr[n0];  // fl|x1 - x2| >= tmax: rejected by the first axis
   for (;;) {
-    unsigned long long idx = 0;
-    if (lane == 0) idx = atomicAdd(A.next_item, 1ull);
-    idx = __shfl_sync(kFull, idx, 0);
-    if (idx >= A.n_items) break;
-    SweepItem it;
-    if (!load_item<COORD>(A, idx, tmax, it)) continue;  // another kernel's item
-    if (grid_item(A, it.i, it.j)) continue;              // the grid sweep's item
-    ++n_taken;
-    if (it.r_hi <= it.r_lo) continue;
-    for (int t0 = 0; t0 < 2 * n0; t0 += 32) run_group<COORD, MINPOS>(A, it, t0, lane, stats);
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(A.next_item, (unsigned long long)kClaimItems);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= A.n_items) break;
+    const unsigned long long mine = base + lane;
+    unsigned todo = __ballot_sync(kFull, mine < A.n_items && item_owner(A, mine) == kOwnerRun);
+    while (todo) {
+      const unsigned long long idx = base + (__ffs(todo) - 1);
+      todo &= todo - 1;
+      SweepItem it;
+      if (!load_item<COORD>(A, idx, tmax, it)) continue;  // another kernel's item
+      if (grid_item(A, it.i, it.j)) continue;              // the grid sweep's item
+      ++n_taken;
+      if (it.r_hi <= it.r_lo) continue;
+      for (int t0 = 0; t0 < 2 * n0; t0 += 32) run_group<COORD, MINPOS>(A, it, t0, lane, stats);
+    }
   }
   add_counters(A, lane, stats[0], stats[1], n_taken, 8);
 }
