@@ -688,6 +688,9 @@ def jackknife_measure(eng, cat, W, plain_step_s, plain_bins):
                    "on the catalogue without that region's sightlines"}
 
 
+SERVE_MAX_WAIT_S = 60.0
+
+
 def serving_measure(W, n_requests, serve_max,
                     runs=(("fifo", 4), ("shortest", 4), ("shortest", 1), ("fifo", 1))):
     """The serving pattern on a resident pool: 6 catalogues whose sightline
@@ -713,11 +716,15 @@ def serving_measure(W, n_requests, serve_max,
     cap = "" if serve_max >= 160000 else f" capped at {serve_max} to bound the bench's time"
     out = {"workload": "pool of 6 resident catalogues (first N sightlines of the full survey, N log-uniform "
                        f"[1k,160k]{cap}), {n_requests} Poisson arrivals at 20/s, binning (r_par,r_perp) "
-                       "50x50 or (r,mu) 50x20 at random, 150 GB budget",
+                       "50x50 or (r,mu) 50x20 at random, 150 GB budget, shortest-first aging limit "
+                       f"{SERVE_MAX_WAIT_S:.0f} s",
            "pool_sightlines": [int(c) for c in counts], "requests": int(n_requests)}
     for policy, slots in runs:
         srv = T.Server(0, slots=slots, memory_budget_bytes=150 * 10**9)
-        srv.set_policy(policy, max_wait_s=5.0)
+        # the aging limit of shortest-first sits above the burst's backlog:
+        # with 5 s every request of a 3 s burst with ~95 s of work ages, and
+        # the order falls back to arrival order
+        srv.set_policy(policy, max_wait_s=SERVE_MAX_WAIT_S)
         eng = T.Engine(0)
         pool = []
         for n in counts:
