@@ -1,5 +1,6 @@
-"""Host-side helpers of the batched configuration (no GPU): merging mock
-catalogues into one catalogue of sightline groups, and the seeded mock draw."""
+"""Host-side helpers of the synthetic catalogues (no GPU): merging mock
+catalogues into one catalogue of sightline groups, the seeded mock draw, and
+the plate layout of the plate-cell tests."""
 import numpy as np
 
 from tos_b200 import synth
@@ -44,3 +45,27 @@ def test_cap_patch_density():
     cap = np.degrees(np.arccos(np.clip(v @ centre, -1, 1))).max()
     # a 25 deg^2 cap has a radius of about 2.82 deg
     assert 2.3 < cap < 3.1
+
+
+def test_plate_tiling_puts_every_sightline_near_its_plate():
+    """BOSS-like plates: ids unique, every sightline on a listed plate whose
+    centre is within 1.5 degrees (a plate's field radius is 1.49 degrees), the
+    nearest one, so the plate-cell tests start from a realistic layout."""
+    import math
+    los, _, _ = small_catalog(n=300, seed=4, size_deg=8.0, max_pixels=4)
+    out, plates = synth.plate_tiling(los, 2.0)
+    assert len(np.unique(plates["plate"])) == len(plates)
+    assert np.isin(out["plate"], plates["plate"]).all()
+    by_id = {int(p["plate"]): p for p in plates}
+
+    def unit(ra, dec):
+        return np.array([math.cos(dec) * math.cos(ra), math.cos(dec) * math.sin(ra), math.sin(dec)])
+
+    for s in range(len(out)):
+        p = by_id[int(out["plate"][s])]
+        u = unit(float(out["ra"][s]), float(out["dec"][s]))
+        d = math.degrees(math.acos(min(1.0, float(u @ unit(math.radians(float(p["ra_center"])),
+                                                            math.radians(float(p["dec_center"])))))))
+        assert d < 1.5, (s, d)
+    # only the plate id changes
+    assert np.array_equal(out["ra"], los["ra"]) and np.array_equal(out["num_pixels"], los["num_pixels"])
