@@ -296,21 +296,27 @@ def reference_arm(args, D):
     from oracle import oracle
     W = make_workload(args.workload, args.sightlines, args.grid)
     nthreads = os.cpu_count() or 1
+    # a step is one bounded sample of the workload (its wall time is the step's)
     if "pts" in W and oracle.ref_available("brute"):
         value, cpu = reference_brute(args, W)
+        n = len(W["pts"])
+        ms_step = n * (n - 1) / 2 / value * 1e3  # mean wall time of a timed call
         dtype = "f32"
     else:
         for _ in range(args.warmup):
             cpu_sample(W, nthreads, max(4, args.cpu_cells // 4))
-        vals = []
+        vals, walls = [], []
         for _ in range(args.steps):
+            t = time.perf_counter()
             v, kind, desc = cpu_sample(W, nthreads, args.cpu_cells)
+            walls.append(time.perf_counter() - t)
             vals.append(v)
         value = float(np.mean(vals))
+        ms_step = float(np.mean(walls)) * 1e3
         cpu = {"value": value, "unit": UNIT, "cores": nthreads, "kind": kind, "sample": desc}
         dtype = "f64"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
             "config": W["config"], "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
