@@ -34,6 +34,24 @@ def test_brute_grid_vs_oracle(engine, n, spacing, rmax, nbins, weights):
     assert np.max(np.abs(ds[nzd] - ods[nzd]) / np.abs(ods[nzd])) < 1e-6
 
 
+@pytest.mark.parametrize("key", ["delta_nanoer", "delta_nano", "delta_micro", "delta_tinier"])
+def test_brute_on_reference_sample_grids(engine, key):
+    """The reference's own sample grids (sample-data/delta-*.dat, 2^3 to 32^3
+    points at 5 Mpc/h), stored with the FP64 oracle's histogram for 100 bins
+    over [0, 200) Mpc/h in tests/golden/golden_brute_sample.npz: separations
+    10, 20, 30 ... Mpc/h fall exactly on bin edges."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_brute_sample.npz"))
+    pts = z[key + "_points"]
+    ds, ws, ct, _ = T.brute_run(engine, pts, float(z["rmin"]), float(z["rmax"]), int(z["nbins"]))
+    assert np.array_equal(ct, z[key + "_counts"]), np.nonzero(ct != z[key + "_counts"])[0][:10]
+    ows, ods = z[key + "_wsum"], z[key + "_dsum"]
+    nz = ows != 0
+    assert np.max(np.abs(ws[nz] - ows[nz]) / np.abs(ows[nz])) < 1e-9
+    nzd = ods != 0
+    assert np.max(np.abs(ds[nzd] - ods[nzd]) / np.abs(ods[nzd])) < 1e-6
+
+
 def test_brute_random_points(engine):
     rng = np.random.default_rng(5)
     pts = np.concatenate([rng.uniform(0, 120, (3000, 3)), rng.normal(size=(3000, 1)),

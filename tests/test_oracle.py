@@ -171,3 +171,42 @@ def test_plate_ring_covers_the_disc_above_1p5_degrees():
             assert pst["num_sightline_pairs_used"] == hst["num_sightline_pairs_used"]
         else:
             assert 0 < pb["num_pairs"].sum() < hb["num_pairs"].sum()
+
+
+def _numpy_brute(pts, rmin, rmax, nbins):
+    """All pairs i < j of the brute-force histogram in FP64 from the float
+    coordinates (gpu/brute.cu:40-48 with bucketxi's double separation):
+    bin 0 below rmin, nbins + 1 at or above rmax."""
+    p = pts.astype(np.float64)
+    spacing = (rmax - rmin) / nbins
+    cnt = np.zeros(nbins + 2, dtype=np.int64)
+    wsum = np.zeros(nbins + 2)
+    for i in range(len(p) - 1):
+        d = p[i + 1:, :3] - p[i, :3]
+        r = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+        k = np.floor((r - rmin) / spacing)
+        idx = np.where(r < rmin, 0, np.where(r >= rmax, nbins + 1, np.minimum(k, nbins - 1) + 1)).astype(np.int64)
+        cnt += np.bincount(idx, minlength=nbins + 2)
+        wsum += np.bincount(idx, weights=p[i, 4] * p[i + 1:, 4], minlength=nbins + 2)
+    return cnt, wsum
+
+
+def test_brute_oracle_on_reference_sample_grids():
+    """The reference's own sample grids (sample-data/delta-*.dat: 2^3 to 32^3
+    points at 5 Mpc/h, kept in tests/golden/golden_brute_sample.npz by
+    make_brute_sample.py): the oracle reproduces the stored histogram, and an
+    independent FP64 pair loop bins the same pairs (many separations, 5 sqrt(k)
+    Mpc/h, fall exactly on the 2 Mpc/h bin edges)."""
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_brute_sample.npz"))
+    rmin, rmax, nbins = float(z["rmin"]), float(z["rmax"]), int(z["nbins"])
+    for key in ("delta_nanoer", "delta_nano", "delta_micro", "delta_tinier"):
+        pts = z[key + "_points"]
+        ds, ws, ct = oracle.brute(pts, rmin, rmax, nbins, nthreads=4)
+        assert np.array_equal(ct, z[key + "_counts"]), key
+        assert int(ct.sum()) == len(pts) * (len(pts) - 1) // 2
+        np.testing.assert_allclose(ws, z[key + "_wsum"], rtol=1e-12)
+        np.testing.assert_allclose(ds, z[key + "_dsum"], rtol=1e-9, atol=1e-9 * np.abs(z[key + "_dsum"]).max())
+        if len(pts) <= 4096:
+            cnt, wsum = _numpy_brute(pts, rmin, rmax, nbins)
+            assert np.array_equal(cnt, ct.astype(np.int64)), key
+            np.testing.assert_allclose(wsum, ws, rtol=1e-12)
