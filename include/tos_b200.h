@@ -163,6 +163,31 @@ tos_status tos_catalog_create_dc(tos_engine* engine, const tos_sightline* los, s
                                  const tos_pixel* pixels, size_t n_pixels, int order, double omega_matter,
                                  tos_catalog** out);
 
+/* One forest as HDF5Delta::loadForests reads it from a group of the delta
+ * file's `lines_of_sight` group (HDF5Delta.cc:52-66): the group's name, its
+ * ra, dec, z and plate attributes, and its delta, weight, r_comov and loglam
+ * datasets of n floats each (z is read by the reference and not used). */
+typedef struct {
+  const char* name;
+  double ra, dec, z;
+  int32_t plate, reserved;
+  uint64_t n;
+  const float *delta, *weight, *r_comov, *loglam;
+} tos_forest;
+
+/* The sightlines and pixels HDF5Delta::loadForests (HDF5Delta.cc:40-93)
+ * builds from those forests, ready for tos_catalog_create: forests in
+ * increasing byte-wise name order (its H5Literate over H5_INDEX_NAME,
+ * increasing); a pixel kept when delta and weight are finite and the weight
+ * is positive, in stored order, as {delta, loglam, weight, r_comov}; forests
+ * left without pixels dropped; forest_id = 0, 1, ... over the kept forests;
+ * ra, dec and plate as given; group 0; pixel ranges contiguous.  Host only
+ * (no device needed).  With los or pixels NULL only *n_los and *n_pixels are
+ * set (size query); otherwise the capacities must hold them. */
+tos_status tos_forests_assemble(const tos_forest* forests, size_t n_forests, tos_sightline* los,
+                                size_t los_capacity, size_t* n_los, tos_pixel* pixels, size_t pixel_capacity,
+                                size_t* n_pixels);
+
 /* One platelist row: the PLATE, RACEN and DECCEN columns (centre in degrees)
  * that PlateBins reads from the platelist FITS file (PlateBins.h:38-45). */
 typedef struct {

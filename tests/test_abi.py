@@ -80,3 +80,65 @@ def test_fill_distances_matches_fp64_integral():
     z = 10.0 ** (px["loglam"].astype(np.float64) - np.log10(1216.0)) - 1.0
     ref = synth.comoving_distance_fp64(z, 0.3)
     assert np.max(np.abs(got - ref) / ref) < 1.2e-7
+
+
+def _loader_restated(forests):
+    """HDF5Delta::loadForests (HDF5Delta.cc:40-93) restated in Python: groups
+    in byte-wise name order, pixels with finite delta and weight and weight
+    > 0, empty forests dropped, forests numbered in that order."""
+    los, px = [], []
+    for f in sorted(forests, key=lambda f: f["name"].encode()):
+        kept = [(d, l, w, r) for d, w, r, l in zip(f["delta"], f["weight"], f["r_comov"], f["loglam"])
+                if np.isfinite(np.float32(d)) and np.isfinite(np.float32(w)) and np.float32(w) > 0]
+        if kept:
+            los.append((f["ra"], f["dec"], len(los), f["plate"], len(px), len(kept), 0))
+            px.extend(kept)
+    return (np.array(los, dtype=T.SIGHTLINE_DTYPE), np.array(px, dtype=T.PIXEL_DTYPE).reshape(-1))
+
+
+def test_forests_assemble_follows_the_loader():
+    rng = np.random.default_rng(12)
+    names = ["10", "9", "B", "a", "a0", "Z", "los-003", "los-001", "los-002", "empty", "allbad"]
+    forests = []
+    for k, name in enumerate(names):
+        n = 0 if name == "empty" else int(rng.integers(1, 40))
+        delta = rng.normal(size=n).astype(np.float32)
+        weight = rng.uniform(0.1, 2, n).astype(np.float32)
+        bad = rng.uniform(size=n) < 0.2
+        delta[bad & (rng.uniform(size=n) < 0.5)] = np.nan
+        weight[bad & (rng.uniform(size=n) < 0.5)] = rng.choice([0.0, -1.0, np.inf, np.nan])
+        if name == "allbad":
+            weight[:] = 0.0
+        forests.append(dict(name=name, ra=0.1 * k, dec=-0.05 * k, z=2.0 + 0.1 * k, plate=3000 + k, delta=delta,
+                            weight=weight, r_comov=rng.uniform(3000, 4000, n).astype(np.float32),
+                            loglam=np.sort(rng.uniform(3.56, 3.74, n)).astype(np.float32)))
+    los, px = T.assemble_forests(forests)
+    rlos, rpx = _loader_restated(forests)
+    assert np.array_equal(los, rlos)
+    assert np.array_equal(px.view(np.uint32), rpx.view(np.uint32))  # bit for bit
+    assert [int(x) for x in los["forest_id"]] == list(range(len(los)))
+    assert len(los) == len(names) - 2  # "empty" and "allbad" are dropped
+
+
+def test_forests_assemble_round_trip_and_capacity():
+    """A catalogue split into named forests comes back unchanged; a buffer
+    that is too small is refused."""
+    import ctypes as C
+    from helpers import small_catalog
+    los0, px0, _ = small_catalog(n=25, seed=4, size_deg=2.0, max_pixels=30)
+    forests = []
+    for s in range(len(los0)):
+        o, n = int(los0[s]["pixel_offset"]), int(los0[s]["num_pixels"])
+        p = px0[o:o + n]
+        forests.append(dict(name=f"{s:06d}", ra=los0[s]["ra"], dec=los0[s]["dec"], plate=int(los0[s]["plate"]),
+                            delta=p["value"], weight=p["weight"], r_comov=p["distance"], loglam=p["loglam"]))
+    los, px = T.assemble_forests(forests[::-1])  # the order given does not matter
+    assert np.array_equal(los, los0) and np.array_equal(px, px0)
+    L = T.lib()
+    arr = (T._Forest * 1)(T._Forest(b"x", 0.0, 0.0, 0.0, 0, 0, 3, *[np.ones(3, np.float32).ctypes.data] * 4))
+    nl, npx = C.c_size_t(), C.c_size_t()
+    small_l = np.zeros(1, dtype=T.SIGHTLINE_DTYPE)
+    small_p = np.zeros(2, dtype=T.PIXEL_DTYPE)
+    st = L.tos_forests_assemble(C.cast(arr, C.c_void_p), 1, small_l.ctypes.data, 1, C.byref(nl),
+                                small_p.ctypes.data, 2, C.byref(npx))
+    assert st == 1 and nl.value == 1 and npx.value == 3  # TOS_ERR_INVALID_ARG, sizes reported

@@ -135,6 +135,7 @@ def lib() -> C.CDLL:
         L.tos_catalog_create_dc.argtypes = [vp, vp, sz, vp, sz, i32, dbl, C.POINTER(vp)]
         L.tos_catalog_distances.argtypes = [vp, vp, sz]
         L.tos_catalog_create_plates.argtypes = [vp, vp, sz, vp, sz, vp, sz, dbl, C.POINTER(vp)]
+        L.tos_forests_assemble.argtypes = [vp, sz, vp, sz, C.POINTER(sz), vp, sz, C.POINTER(sz)]
         for name in ("tos_engine_create", "tos_catalog_create", "tos_catalog_num_cells", "tos_catalog_cells",
                      "tos_catalog_sightline_cells", "tos_grid_max_angular_scale", "tos_xi_run",
                      "tos_brute_run", "tos_brute_tune", "tos_comoving_distance", "tos_fill_distances"):
@@ -546,6 +547,40 @@ def fill_distances(omega_matter: float, pixels: np.ndarray) -> np.ndarray:
     out = np.ascontiguousarray(pixels, dtype=PIXEL_DTYPE).copy()
     _check(lib().tos_fill_distances(omega_matter, _ptr(out), len(out)))
     return out
+
+
+class _Forest(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("ra", C.c_double), ("dec", C.c_double), ("z", C.c_double),
+                ("plate", C.c_int32), ("reserved", C.c_int32), ("n", C.c_uint64),
+                ("delta", C.c_void_p), ("weight", C.c_void_p), ("r_comov", C.c_void_p), ("loglam", C.c_void_p)]
+
+
+def assemble_forests(forests):
+    """Sightlines and pixels (SIGHTLINE_DTYPE, PIXEL_DTYPE arrays) from forests
+    as HDF5Delta::loadForests reads them (tos_forests_assemble): forests is a
+    sequence of dicts with the group's name, its ra, dec, z and plate
+    attributes and its delta, weight, r_comov and loglam datasets."""
+    keep = []
+    arr = (_Forest * max(1, len(forests)))()
+    for k, f in enumerate(forests):
+        cols = [np.ascontiguousarray(f[c], dtype=np.float32) for c in ("delta", "weight", "r_comov", "loglam")]
+        n = len(cols[0])
+        if any(len(c) < n for c in cols[1:]):
+            raise ValueError(f"forest {f['name']!r}: datasets shorter than delta")
+        name = f["name"].encode() if isinstance(f["name"], str) else bytes(f["name"])
+        keep.append((name, cols))
+        arr[k] = _Forest(name, float(f["ra"]), float(f["dec"]), float(f.get("z", 0.0)), int(f.get("plate", 0)), 0,
+                         n, *[c.ctypes.data for c in cols])
+    n_los, n_px = C.c_size_t(), C.c_size_t()
+    L = lib()
+    arr = C.cast(arr, C.c_void_p)
+    _check(L.tos_forests_assemble(arr, len(forests), None, 0, C.byref(n_los), None, 0, C.byref(n_px)))
+    los = np.zeros(max(1, n_los.value), dtype=SIGHTLINE_DTYPE)
+    px = np.zeros(max(1, n_px.value), dtype=PIXEL_DTYPE)
+    _check(L.tos_forests_assemble(arr, len(forests), _ptr(los), len(los), C.byref(n_los), _ptr(px), len(px),
+                                  C.byref(n_px)))
+    del keep
+    return los[:n_los.value], px[:n_px.value]
 
 
 def comoving_distance(omega_matter: float, z) -> np.ndarray:
